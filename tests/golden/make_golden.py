@@ -1,0 +1,427 @@
+"""Generate the golden fixtures in this folder by running the reference's own kernels.
+
+The reference (kuiwuchn/OpenHOMELBM) is Python whose GPU work is NVIDIA Warp kernels. Warp
+is not installable here, so this script installs ``warp_emu`` (a CPU emulation of the Warp
+builtins those kernels call) as the ``warp`` module, imports the reference's kernel modules
+from their source tree, and launches the kernels in the order the reference's solvers
+launch them:
+
+* 2D, ``LBM_Solver.step`` (envs/lbm/lbm_solver.py:104-141): zero the per-solid loads,
+  ``precompute_transformed_segments`` -> ``stream_and_collide`` -> ``apply_bc`` ->
+  ``Swap_Mom``; prescribed solid motion through ``advance_prescribed_solid_motion_kernel``
+  (envs/lbm/karman/karman_lbm_env.py:65-77) before each step.
+* 3D, ``LBM_Solver3D.step`` (envs/lbm3d/lbm_solver_3d.py:95-127): ``init_force_3d_batch``
+  -> ``stream_and_collide_3d`` -> ``apply_bc_3d`` -> ``Swap_Mom_3D``; poses enter through
+  ``convert_and_update_solid_batch_3d`` (envs/lbm3d/lbm_fluid_env_3d_func.py:42-100).
+* 3D periodic: the reference has no periodic boundary, so the periodic case runs the
+  reference kernel on an (n+2)^3 grid whose ghost shell is WALL and is refilled with the
+  periodic images of the interior after every ``stream_and_collide_3d`` (no ``apply_bc_3d``).
+
+Usage (needs the reference source tree; the fixtures it writes are committed):
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import warp_emu  # noqa: E402
+
+
+def import_reference(ref):
+    wp = warp_emu.install()
+
+    def pkg(name, path):
+        m = types.ModuleType(name)
+        m.__path__ = [path]
+        sys.modules[name] = m
+        return m
+
+    pkg("refenvs", f"{ref}/envs")
+    pkg("refenvs.lbm", f"{ref}/envs/lbm")
+    pkg("refenvs.lbm3d", f"{ref}/envs/lbm3d")
+    pkg("refenvs.lbm.karman", f"{ref}/envs/lbm/karman")
+    # the gym environment base class is not needed by the kernels; stand it in
+    stub = types.ModuleType("refenvs.lbm.lbm_fluid_env")
+    stub.LBMFluidEnv = object
+    sys.modules["refenvs.lbm.lbm_fluid_env"] = stub
+    mods = types.SimpleNamespace(wp=wp)
+    mods.core2 = importlib.import_module("refenvs.lbm.lbm_core")
+    mods.func2 = importlib.import_module("refenvs.lbm.lbm_func")
+    mods.solid = importlib.import_module("refenvs.lbm.solid_func")
+    mods.karman2 = importlib.import_module("refenvs.lbm.karman.karman_lbm_env")
+    mods.couple2 = importlib.import_module("refenvs.lbm.lbm_fluid_env_func")
+    mods.core3 = importlib.import_module("refenvs.lbm3d.lbm_core_3d")
+    mods.func3 = importlib.import_module("refenvs.lbm3d.lbm_func_3d")
+    mods.couple3 = importlib.import_module("refenvs.lbm3d.lbm_fluid_env_3d_func")
+    return mods
+
+
+# --------------------------------------------------------------------------- 2D
+def _moments2d(flow):
+    return np.stack([flow.rho.np, flow.u.np[..., 0], flow.u.np[..., 1],
+                     flow.Sxx.np, flow.Syy.np, flow.Sxy.np]).astype(np.float32)
+
+
+def _set_moments2d(flow, m):
+    for cur, post in ((flow.rho, flow.rho_post), (flow.Sxx, flow.Sxx_post),
+                      (flow.Syy, flow.Syy_post), (flow.Sxy, flow.Sxy_post)):
+        pass
+    flow.rho.np[...] = m[0]
+    flow.u.np[..., 0] = m[1]
+    flow.u.np[..., 1] = m[2]
+    flow.Sxx.np[...] = m[3]
+    flow.Syy.np[...] = m[4]
+    flow.Sxy.np[...] = m[5]
+    flow.rho_post.np[...] = m[0]
+    flow.u_post.np[..., 0] = m[1]
+    flow.u_post.np[..., 1] = m[2]
+    flow.Sxx_post.np[...] = m[3]
+    flow.Syy_post.np[...] = m[4]
+    flow.Sxy_post.np[...] = m[5]
+
+
+def case_2d(R, name, nx, ny, steps, seed, vis, bc_type, bc_value, solids, motion, init,
+            force_amp):
+    wp = R.wp
+    rng = np.random.default_rng(seed)
+    flow = R.core2.HomeFlow()
+    flow.Initialize(nx, ny, n_objects=max(1, len(solids)))
+    flow.vis_shear = vis
+    flow.bc_type = wp.types.vector(length=4, dtype=wp.int32)(*bc_type)
+    flow.bc_value = wp.array(tuple(wp.vec2(*v) for v in bc_value), dtype=wp.vec2)
+    for sid, s in enumerate(solids):
+        flow.configure_solid(sid, np.asarray(s["lines"], np.float32), tuple(s["position"]),
+                             angle=s["angle"], scale=s["scale"])
+    flows = wp.array([flow], dtype=R.core2.HomeFlow)
+    wp.launch(R.func2.InitBoundary, dim=(1, nx, ny), inputs=[flows])
+    if init == "uniform":
+        ux, uy = bc_value[0]
+        wp.launch(R.karman2.set_uniform_flow_kernel, dim=(1, nx, ny), inputs=[flows, ux, uy])
+        noise = rng.uniform(-1e-3, 1e-3, size=(nx, ny, 2)).astype(np.float32)
+        flow.u.np[...] += noise
+        flow.u_post.np[...] = flow.u.np
+    else:
+        wp.launch(R.func2.InitFlow, dim=(1, nx, ny), inputs=[flows])
+        m = np.empty((6, nx, ny), np.float32)
+        m[0] = 1.0 + rng.uniform(-0.01, 0.01, (nx, ny))
+        m[1] = rng.uniform(-0.04, 0.04, (nx, ny))
+        m[2] = rng.uniform(-0.04, 0.04, (nx, ny))
+        m[3] = m[1] * m[1] + rng.uniform(-2e-3, 2e-3, (nx, ny))
+        m[4] = m[2] * m[2] + rng.uniform(-2e-3, 2e-3, (nx, ny))
+        m[5] = m[1] * m[2] + rng.uniform(-2e-3, 2e-3, (nx, ny))
+        _set_moments2d(flow, m.astype(np.float32))
+    if force_amp:
+        flow.forcex.np[...] = rng.uniform(-force_amp, force_amp, (nx, ny)).astype(np.float32)
+        flow.forcey.np[...] = rng.uniform(-force_amp, force_amp, (nx, ny)).astype(np.float32)
+
+    out = {
+        "nx": nx, "ny": ny, "vis_shear": np.float32(vis), "steps": steps,
+        "bc_type": np.array(bc_type, np.int32), "bc_value": np.array(bc_value, np.float32),
+        "init_moments": _moments2d(flow), "flag": flow.flag.np.copy(),
+        "forcex": flow.forcex.np.copy(), "forcey": flow.forcey.np.copy(),
+        "n_objects": flow.n_objects, "max_segments": flow.max_segments_per_object,
+        "solid_line": flow.solid_line.np.copy(), "solid_line_num": flow.solid_line_num.np.copy(),
+        "solid_position0": flow.solid_position.np.copy(), "solid_angle0": flow.solid_angle.np.copy(),
+        "solid_scale": flow.solid_scale.np.copy(), "solid_mass_center": flow.solid_mass_center.np.copy(),
+        "solid_max_radius": flow.solid_max_radius.np.copy(),
+        "motion": np.array(motion if motion else [0.0, 0.0, 0.0], np.float32),
+        "grid_length": np.float32(flow.grid_length), "time_step": np.float32(flow.time_step),
+    }
+    moments, forces, tfs, tfls = [], [], [], []
+    for step in range(steps):
+        if motion:
+            wp.launch(R.karman2.advance_prescribed_solid_motion_kernel, dim=1,
+                      inputs=[flows, 0, motion[0], motion[1], motion[2]])
+        R.func2.init_force(flow)
+        wp.launch(R.func2.precompute_transformed_segments,
+                  dim=(1, flow.n_objects, flow.max_segments_per_object), inputs=[flows])
+        wp.launch(R.func2.stream_and_collide, dim=(1, nx, ny), inputs=[flows])
+        wp.launch(R.func2.apply_bc, dim=(1, nx, ny), inputs=[flows])
+        wp.launch(R.func2.Swap_Mom, dim=(1,), inputs=[flows])
+        moments.append(_moments2d(flow))
+        forces.append(np.stack([flow.solid_forcex.np, flow.solid_forcey.np, flow.torque.np]).copy())
+        tfs.append(flow.solid_line_transformed.np.copy())
+        tfls.append(flow.solid_line_transformed_last.np.copy())
+    out["moments"] = np.stack(moments)
+    out["solid_loads"] = np.stack(forces)
+    out["solid_line_transformed"] = np.stack(tfs)
+    out["solid_line_transformed_last"] = np.stack(tfls)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(f"{name}: {steps} steps, moments finite={np.isfinite(out['moments']).all()}, "
+          f"loads={out['solid_loads'][-1].ravel()[:3]}")
+
+
+# --------------------------------------------------------------------------- 3D
+_FIELDS3 = ["rho", "ux", "uy", "uz", "Sxx", "Syy", "Szz", "Sxy", "Sxz", "Syz"]
+
+
+def _moments3d(flow, post=False):
+    sfx = "_post" if post else ""
+    u = getattr(flow, "u" + sfx).np
+    return np.stack([getattr(flow, "rho" + sfx).np, u[..., 0], u[..., 1], u[..., 2]] +
+                    [getattr(flow, n + sfx).np for n in ("Sxx", "Syy", "Szz", "Sxy", "Sxz", "Syz")]
+                    ).astype(np.float32)
+
+
+def _set_moments3d(flow, m):
+    for sfx in ("", "_post"):
+        getattr(flow, "rho" + sfx).np[...] = m[0]
+        u = getattr(flow, "u" + sfx).np
+        u[..., 0], u[..., 1], u[..., 2] = m[1], m[2], m[3]
+        for k, n in enumerate(("Sxx", "Syy", "Szz", "Sxy", "Sxz", "Syz")):
+            getattr(flow, n + sfx).np[...] = m[4 + k]
+
+
+def _random_moments3d(rng, shape):
+    m = np.empty((10,) + shape, np.float32)
+    m[0] = 1.0 + rng.uniform(-0.01, 0.01, shape)
+    for k in range(3):
+        m[1 + k] = rng.uniform(-0.04, 0.04, shape)
+    pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2)]
+    for k, (a, b) in enumerate(pairs):
+        m[4 + k] = m[1 + a] * m[1 + b] + rng.uniform(-2e-3, 2e-3, shape)
+    return m.astype(np.float32)
+
+
+def _octahedron(radius):
+    v = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]],
+                 np.float32) * radius
+    f = np.array([[0, 2, 4], [2, 1, 4], [1, 3, 4], [3, 0, 4],
+                  [2, 0, 5], [1, 2, 5], [3, 1, 5], [0, 3, 5]], np.int32)
+    return v, f
+
+
+def _quat_wxyz(axis, angle):
+    axis = np.asarray(axis, np.float64)
+    axis = axis / np.linalg.norm(axis)
+    h = 0.5 * angle
+    return np.array([np.cos(h), *(np.sin(h) * axis)], np.float32)
+
+
+def case_3d(R, name, shape, steps, seed, vis, bc_type, bc_value, periodic=False,
+            mesh=None, force_amp=0.0):
+    wp = R.wp
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = shape
+    gx, gy, gz = (nx + 2, ny + 2, nz + 2) if periodic else (nx, ny, nz)
+    n_obj = 1
+    flow = R.core3.HomeFlow3D()
+    flow.Initialize(gx, gy, gz, n_objects=n_obj)
+    flow.vis_shear = vis
+    flow.bc_type = wp.types.vector(length=6, dtype=wp.int32)(*bc_type)
+    flow.bc_value = wp.array(tuple(wp.vec3(*v) for v in bc_value), dtype=wp.vec3)
+    flows = wp.array([flow], dtype=R.core3.HomeFlow3D)
+    wp.launch(R.func3.InitBoundary3D, dim=(1, gx, gy, gz), inputs=[flows])
+    wp.launch(R.func3.InitFlow3D, dim=(1, gx, gy, gz), inputs=[flows])
+    m = _random_moments3d(rng, (nx, ny, nz))
+    if periodic:
+        full = np.pad(m, ((0, 0), (1, 1), (1, 1), (1, 1)), mode="wrap")
+        _set_moments3d(flow, full)
+    else:
+        _set_moments3d(flow, m)
+    if force_amp:
+        for c in ("forcex", "forcey", "forcez"):
+            f = rng.uniform(-force_amp, force_amp, (nx, ny, nz)).astype(np.float32)
+            getattr(flow, c).np[...] = np.pad(f, 1, mode="wrap") if periodic else f
+
+    mesh_info = None
+    poses = []
+    if mesh is not None:
+        verts, faces = _octahedron(mesh["radius"])
+        m_wp = wp.Mesh(points=wp.array(verts, dtype=wp.vec3), indices=wp.array(faces.ravel(), dtype=wp.int32))
+        flow.mesh_ids.np[0] = m_wp.id
+        flow.mesh_scale_sizes.np[0] = (1.0, 1.0, 1.0)
+        flow.solid_bound_radius.np[0] = float(np.linalg.norm(verts, axis=1).max())
+        mesh_info = (verts, faces)
+        for s in range(steps):
+            pos = np.asarray(mesh["position"], np.float32) + np.asarray(mesh["velocity"], np.float32) * s
+            q = _quat_wxyz(mesh["axis"], mesh["omega"] * s)
+            poses.append((pos.astype(np.float32), q))
+
+    out = {"shape": np.array(shape, np.int32), "periodic": int(periodic), "steps": steps,
+           "vis_shear": np.float32(vis), "bc_type": np.array(bc_type, np.int32),
+           "bc_value": np.array(bc_value, np.float32), "init_moments": m,
+           "force": (np.stack([flow.forcex.np, flow.forcey.np, flow.forcez.np])[:, 1:-1, 1:-1, 1:-1]
+                     if periodic else np.stack([flow.forcex.np, flow.forcey.np, flow.forcez.np])).copy()}
+    if mesh_info is not None:
+        out["mesh_vertices"], out["mesh_faces"] = mesh_info
+        out["bound_radius"] = flow.solid_bound_radius.np.copy()
+        out["poses_pos"] = np.stack([p for p, _ in poses])
+        out["poses_quat_wxyz"] = np.stack([q for _, q in poses])
+    moments, loads, tfs = [], [], []
+    solid_ids = wp.array(np.array([0], np.int32), dtype=wp.int32)
+    ones = wp.array(np.array([1.0], np.float32), dtype=wp.float32)
+    zero3 = wp.array(np.zeros((1, 3), np.float32), dtype=wp.vec3)
+    for step in range(steps):
+        if mesh is not None:
+            pos, q = poses[step]
+            mj_pos = wp.array(pos.reshape(1, 1, 3), dtype=wp.float32)
+            mj_quat = wp.array(q.reshape(1, 1, 4), dtype=wp.float32)
+            wp.launch(R.couple3.convert_and_update_solid_batch_3d, dim=(1, 1),
+                      inputs=[flows, solid_ids, mj_pos, mj_quat, zero3, zero3, ones])
+            tfs.append(np.stack([flow.mesh_transforms.np[0], flow.mesh_transforms_last.np[0]]).copy())
+        wp.launch(R.func3.init_force_3d_batch, dim=(1,), inputs=[flows])
+        wp.launch(R.func3.stream_and_collide_3d, dim=(1, gx, gy, gz), inputs=[flows])
+        if periodic:
+            post = _moments3d(flow, post=True)
+            interior = post[:, 1:-1, 1:-1, 1:-1]
+            _set_post3d(flow, np.pad(interior, ((0, 0), (1, 1), (1, 1), (1, 1)), mode="wrap"))
+        else:
+            wp.launch(R.func3.apply_bc_3d, dim=(1, gx, gy, gz), inputs=[flows])
+        wp.launch(R.func3.Swap_Mom_3D, dim=(1,), inputs=[flows])
+        cur = _moments3d(flow)
+        moments.append(cur[:, 1:-1, 1:-1, 1:-1] if periodic else cur)
+        loads.append(np.concatenate([flow.solid_force.np[0], flow.solid_torque.np[0]]).copy())
+    out["moments"] = np.stack(moments)
+    out["solid_loads"] = np.stack(loads)
+    if tfs:
+        out["transforms"] = np.stack(tfs)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(f"{name}: {steps} steps, finite={np.isfinite(out['moments']).all()}, loads={out['solid_loads'][-1]}")
+
+
+def _set_post3d(flow, m):
+    flow.rho_post.np[...] = m[0]
+    u = flow.u_post.np
+    u[..., 0], u[..., 1], u[..., 2] = m[1], m[2], m[3]
+    for k, n in enumerate(("Sxx", "Syy", "Szz", "Sxy", "Sxz", "Syz")):
+        getattr(flow, n + "_post").np[...] = m[4 + k]
+
+
+# --------------------------------------------------------------------------- coupling
+def case_coupling(R, name, seed):
+    """Pose-in and load-out kernels of both coupled environments on random buffers."""
+    wp = R.wp
+    rng = np.random.default_rng(seed)
+    nworld, nbody, nsol = 2, 5, 3
+    body_ids = np.array([1, 3, 4], np.int32)
+    xipos = rng.uniform(-1, 1, (nworld, nbody, 3)).astype(np.float32)
+    q = rng.normal(size=(nworld, nbody, 4))
+    xquat = (q / np.linalg.norm(q, axis=-1, keepdims=True)).astype(np.float32)
+    mj_origin = rng.uniform(-0.5, 0.5, (nsol, 3)).astype(np.float32)
+    lbm_origin = rng.uniform(10, 20, (nsol, 3)).astype(np.float32)
+    scales = rng.uniform(20, 40, (nsol,)).astype(np.float32)
+
+    pos_out = wp.zeros((nworld, nsol, 3), dtype=wp.float32)
+    quat_out = wp.zeros((nworld, nsol, 4), dtype=wp.float32)
+    wp.launch(R.couple3.extract_body_states_3d, dim=(nworld, nsol),
+              inputs=[wp.array(xipos, dtype=wp.vec3), wp.array(xquat, dtype=wp.quat),
+                      wp.array(body_ids, dtype=wp.int32), pos_out, quat_out])
+
+    flows3 = []
+    for _ in range(nworld):
+        f = R.core3.HomeFlow3D()
+        f.Initialize(6, 6, 6, n_objects=nsol)
+        f.solid_force.np[...] = rng.uniform(-1, 1, (nsol, 3))
+        f.solid_torque.np[...] = rng.uniform(-1, 1, (nsol, 3))
+        flows3.append(f)
+    fw3 = wp.array(flows3, dtype=R.core3.HomeFlow3D)
+    sids = wp.array(np.arange(nsol, dtype=np.int32), dtype=wp.int32)
+    tf_hist = []
+    for _ in range(2):  # first call initialises, second moves current -> last
+        wp.launch(R.couple3.convert_and_update_solid_batch_3d, dim=(nworld, nsol),
+                  inputs=[fw3, sids, pos_out, quat_out, wp.array(mj_origin, dtype=wp.vec3),
+                          wp.array(lbm_origin, dtype=wp.vec3), wp.array(scales, dtype=wp.float32)])
+        tf_hist.append(np.stack([np.stack([f.mesh_transforms.np, f.mesh_transforms_last.np])
+                                 for f in flows3]))
+        pos_out.np[...] += np.float32(0.01)
+    fo = wp.zeros((nworld, nsol, 3), dtype=wp.float32)
+    to = wp.zeros((nworld, nsol, 3), dtype=wp.float32)
+    wp.launch(R.couple3.extract_forces_torques_physical_3d, dim=(nworld, nsol),
+              inputs=[fw3, sids, 1.7, 0.3, fo, to])
+    xfrc = wp.zeros((nworld, nbody), dtype=wp.spatial_vector)
+    wp.launch(R.couple3.fill_xfrc_3d_kernel, dim=(nworld, nsol),
+              inputs=[xfrc, wp.array(body_ids, dtype=wp.int32), fo, to])
+
+    flows2 = []
+    for _ in range(nworld):
+        f = R.core2.HomeFlow()
+        f.Initialize(6, 6, n_objects=nsol)
+        f.solid_forcex.np[...] = rng.uniform(-1, 1, nsol)
+        f.solid_forcey.np[...] = rng.uniform(-1, 1, nsol)
+        f.torque.np[...] = rng.uniform(-1, 1, nsol)
+        flows2.append(f)
+    fw2 = wp.array(flows2, dtype=R.core2.HomeFlow)
+    wp.launch(R.couple2.convert_and_update_solid_batch_2d, dim=(nworld, nsol),
+              inputs=[fw2, sids, pos_out, quat_out, wp.array(mj_origin[:, :2], dtype=wp.float32),
+                      wp.array(lbm_origin[:, :2], dtype=wp.float32), wp.array(scales, dtype=wp.float32)])
+    fo2 = wp.zeros((nworld, nsol, 3), dtype=wp.float32)
+    to2 = wp.zeros((nworld, nsol, 3), dtype=wp.float32)
+    wp.launch(R.couple2.extract_forces_torques_batch, dim=(nworld, nsol),
+              inputs=[fw2, sids, wp.array(scales, dtype=wp.float32), fo2, to2])
+    xfrc2 = wp.zeros((nworld, nbody), dtype=wp.spatial_vector)
+    wp.launch(R.couple2.fill_xfrc_kernel, dim=(nworld, nsol),
+              inputs=[xfrc2, wp.array(body_ids, dtype=wp.int32), fo2, to2])
+
+    np.savez_compressed(
+        os.path.join(HERE, f"{name}.npz"),
+        body_ids=body_ids, xipos=xipos, xquat=xquat, mj_origin=mj_origin, lbm_origin=lbm_origin,
+        scales=scales, pos_out=pos_out.np, quat_out=quat_out.np,
+        tf_hist=np.stack(tf_hist), pos_after=pos_out.np.copy(),
+        solid_force3=np.stack([f.solid_force.np for f in flows3]),
+        solid_torque3=np.stack([f.solid_torque.np for f in flows3]),
+        force_conv=np.float32(1.7), torque_conv=np.float32(0.3),
+        forces3=fo.np, torques3=to.np, xfrc3=xfrc.np,
+        solid_position2=np.stack([f.solid_position.np for f in flows2]),
+        solid_angle2=np.stack([f.solid_angle.np for f in flows2]),
+        loads2=np.stack([np.stack([f.solid_forcex.np, f.solid_forcey.np, f.torque.np]) for f in flows2]),
+        forces2=fo2.np, torques2=to2.np, xfrc2=xfrc2.np)
+    print(f"{name}: ok")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("HOMELBM_REFERENCE", "/root/reference"))
+    ap.add_argument("--only", default=None)
+    args = ap.parse_args()
+    R = import_reference(args.reference)
+    circle = np.asarray(R.solid.generate_unit_circle_points(24), np.float32)
+    square = np.array([[-1, -1], [1, -1], [1, 1], [-1, 1]], np.float32)
+    cases = {
+        "d2q9_walls": lambda: case_2d(
+            R, "d2q9_walls", 20, 12, 4, 11, 0.02, [0, 1, 1, 1],
+            [[0.05, 0.01], [0.0, 0.0], [0.0, 0.0], [0.0, 0.0]], [], None, "random", 1e-4),
+        "d2q9_bc_types": lambda: case_2d(
+            R, "d2q9_bc_types", 14, 17, 4, 12, 0.05, [1, 0, 0, 2],
+            [[0.0, 0.0], [0.03, -0.01], [-0.02, 0.02], [0.0, 0.0]], [], None, "random", 0.0),
+        "d2q9_solids": lambda: case_2d(
+            R, "d2q9_solids", 36, 22, 6, 13, 0.03, [0, 1, 1, 1],
+            [[0.04, 0.0], [0.0, 0.0], [0.0, 0.0], [0.0, 0.0]],
+            [dict(lines=circle, position=(11.3, 10.7), angle=0.0, scale=3.6 / 36),
+             dict(lines=square, position=(24.6, 12.2), angle=0.3, scale=2.5 / 36)],
+            [0.02, -0.01, 0.03], "uniform", 0.0),
+        "d3q27_walls": lambda: case_3d(
+            R, "d3q27_walls", (8, 7, 9), 3, 21, 0.05, [0, 1, 1, 0, 1, 2],
+            [[0.03, 0.0, 0.01], [0, 0, 0], [0, 0, 0], [0.0, -0.02, 0.01], [0, 0, 0], [0, 0, 0]],
+            force_amp=1e-4),
+        "d3q27_periodic": lambda: case_3d(
+            R, "d3q27_periodic", (6, 5, 7), 3, 22, 0.04, [1] * 6, [[0, 0, 0]] * 6, periodic=True,
+            force_amp=1e-4),
+        "d3q27_mesh": lambda: case_3d(
+            R, "d3q27_mesh", (12, 11, 12), 3, 23, 0.05, [0, 1, 1, 1, 1, 1],
+            [[0.03, 0.0, 0.0]] + [[0, 0, 0]] * 5,
+            mesh=dict(radius=2.6, position=(5.7, 5.2, 6.1), velocity=(0.05, 0.02, -0.03),
+                      axis=(0.3, 1.0, 0.2), omega=0.05)),
+        "coupling": lambda: case_coupling(R, "coupling", 31),
+    }
+    for k, fn in cases.items():
+        if args.only and k not in args.only.split(","):
+            continue
+        fn()
+    with open(os.path.join(HERE, "MANIFEST.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py",
+                   "cases": sorted(cases)}, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()
