@@ -1,0 +1,344 @@
+"""Benchmark of the HOME-LBM D3Q27 step on B200: MLUPS and fraction of the HBM roofline.
+
+Workload: the 3D Taylor-Green vortex, periodic 256^3 box, FP32 moment storage, u0 = 0.04,
+Re = 1600 (nu = u0 (256/2pi) / 1600). One step = one stream-collide of the whole domain.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 256]
+
+Prints one JSON line (rank 0). Under torchrun each rank steps its own replica of the
+domain (the worlds of the reference never interact, so the path shards without a
+collective); the timed region is bracketed by a barrier and device synchronisation and the
+slowest rank's time is used.
+
+``--impl reference`` times the reference algorithm on the host cores instead: the
+reference is Python + NVIDIA Warp, Warp is not installable on this machine, so the CPU arm
+runs the C++ restatement of the reference kernels (oracle/, all host threads) on a bounded
+slab of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "D3Q27 MLUPS (256^3 periodic Taylor-Green, FP32)"
+UNIT = "MLUPS"
+BYTES_PER_CELL = {"float32": 80, "float16": 40, "bfloat16": 40, "float64": 160}
+
+
+# ----------------------------------------------------------------------------- helpers
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(n, storage):
+    """dram bytes per launch of the stream-collide kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "d3q27_stream_collide_traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    rec = d.get(storage)
+    if not rec:
+        return None
+    # traffic scales with the cells a launch processes
+    return float(rec["dram_bytes_per_cell"]) * n ** 3
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(n_yz, budget_s=12.0, nthreads=0):
+    """The oracle (C++ restatement of the reference kernels, all host threads) on a periodic
+    slab of the workload's cross-section; returns MLUPS and the sample description."""
+    from oracle import oracle as orc
+
+    threads = nthreads or orc.max_threads()
+    nx = 8
+    u0 = 0.04
+    x = 2 * np.pi * np.arange(n_yz) / n_yz
+    Y, Z = np.meshgrid(x, x, indexing="ij")
+    X = (2 * np.pi * np.arange(nx) / n_yz)[:, None, None]
+    ux = u0 * np.sin(X) * np.cos(Y) * np.cos(Z)
+    uy = -u0 * np.cos(X) * np.sin(Y) * np.cos(Z)
+    uz = np.zeros_like(ux)
+    rho = 1 + 3 * (u0 ** 2 / 16) * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2)
+    m = np.stack([rho, ux, uy, uz, ux * ux, uy * uy, uz * uz, ux * uy, ux * uz, uy * uz]).astype(np.float32)
+    prev = m.copy()
+    vis = np.float32(u0 * (n_yz / (2 * np.pi)) / 1600.0)
+    orc.step_3d(m, prev, vis_shear=vis, periodic=True, nthreads=threads)  # warm-up
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        new, _ = orc.step_3d(m, prev, vis_shear=vis, periodic=True, nthreads=threads)
+        m, prev = new, m
+        steps += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    cells = nx * n_yz * n_yz
+    return {"value": cells * steps / dt / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} steps of a periodic {nx}x{n_yz}x{n_yz} slab of the workload "
+                      f"({dt:.1f} s, C++ restatement of stream_and_collide_3d, not Warp)"}
+
+
+# ----------------------------------------------------------------------------- arms
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from oracle import oracle as orc
+
+    threads = orc.max_threads()
+    n = args.n
+    nx = 4
+    u0 = 0.04
+    x = 2 * np.pi * np.arange(n) / n
+    Y, Z = np.meshgrid(x, x, indexing="ij")
+    X = (2 * np.pi * np.arange(nx) / n)[:, None, None]
+    ux = u0 * np.sin(X) * np.cos(Y) * np.cos(Z)
+    uy = -u0 * np.cos(X) * np.sin(Y) * np.cos(Z)
+    z0 = np.zeros_like(ux)
+    rho = 1 + 3 * (u0 ** 2 / 16) * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2)
+    m = np.stack([rho, ux, uy, z0, ux * ux, uy * uy, z0, ux * uy, z0, z0]).astype(np.float32)
+    prev = m.copy()
+    vis = np.float32(u0 * (n / (2 * np.pi)) / 1600.0)
+    for _ in range(args.warmup):
+        new, _ = orc.step_3d(m, prev, vis_shear=vis, periodic=True, nthreads=threads)
+        m, prev = new, m
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        new, _ = orc.step_3d(m, prev, vis_shear=vis, periodic=True, nthreads=threads)
+        m, prev = new, m
+    dt = time.perf_counter() - t0
+    cells = nx * n * n
+    value = cells * args.steps / dt / 1e6
+    sample = (f"each step is one stream-collide of a periodic {nx}x{n}x{n} slab of the {n}^3 workload "
+              f"(C++ restatement of the reference's stream_and_collide_3d; Warp is not installable here)")
+    return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (Taylor-Green initial state)",
+            "config": {"workload": f"D3Q27 Taylor-Green vortex {n}^3 periodic, FP32", "u0": u0,
+                       "Re": 1600, "sample_cells": cells},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+
+    from openhomelbm_b200 import _lib
+    from openhomelbm_b200.lbm3d import LBM_Solver3D
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    n = args.n
+    storage = args.storage
+    u0 = 0.04
+    vis = u0 * (n / (2 * np.pi)) / 1600.0
+    s = LBM_Solver3D(n, n, n, solid_num=1, periodic=True, storage=storage, device=dev,
+                     u_scale=u0, s_scale=u0 * u0 * 0.05)
+    s.set_viscosity(vis)
+    s.init_tgv(u0)
+    f = s.flows[0]
+    cells = n ** 3
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---------------------------------------------------------------- device-resident timing
+    for _ in range(max(args.warmup, 3)):
+        s.step()
+    barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        barrier()
+        start.record(stream)
+        for _ in range(args.steps):
+            s.step()
+        end.record(stream)
+        barrier()
+    ms = start.elapsed_time(end)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * cells * args.steps / (ms / 1e3) / 1e6
+
+    # ---------------------------------------------------------------- end to end, host buffers
+    # The job's input field comes from pinned host memory and its final field goes back to
+    # pinned host memory inside the timed region; every step also reads back its mass and
+    # health words (the per-step result a caller watches). Steps go through LBM_Solver3D.step.
+    init_host = f.cur.detach().to("cpu").pin_memory()
+    out_host = torch.empty_like(init_host).pin_memory()
+    mass_host = torch.empty(args.steps, dtype=torch.float64).pin_memory()
+    health_host = torch.empty(args.steps, dtype=torch.int32).pin_memory()
+    s.diagnostics = True
+    s.step()
+    barrier()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e_start.record(stream)
+    f.cur.copy_(init_host, non_blocking=True)
+    for k in range(args.steps):
+        s.step()
+        mass_host[k:k + 1].copy_(s.mass[0:1], non_blocking=True)
+        health_host[k:k + 1].copy_(s.health[0:1], non_blocking=True)
+    out_host.copy_(f.cur, non_blocking=True)
+    e_end.record(stream)
+    barrier()
+    e_ms = e_start.elapsed_time(e_end)
+    if dist is not None:
+        t = torch.tensor([e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    e2e = world * cells * args.steps / (e_ms / 1e3) / 1e6
+    field_bytes = init_host.numel() * init_host.element_size()
+    health = int(health_host.max().item())
+    s.diagnostics = False
+
+    if rank != 0:
+        return None
+    peak, peak_kind = measured_peaks()
+    bpc = BYTES_PER_CELL[storage]
+    achieved = bpc * cells / (ms_step / 1e3) / 1e9
+    traffic = profile_traffic(n, storage)
+    out = {
+        "metric": METRIC if storage == "float32" else METRIC.replace("FP32", storage),
+        "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (Taylor-Green initial state)",
+        "config": {"workload": f"D3Q27 Taylor-Green vortex {n}^3 periodic, {storage} storage, one stream-collide "
+                               f"per step", "u0": u0, "Re": 1600, "vis_shear": vis,
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 "
+                   f"({cells * bpc / 1e9:.2f} GB moved per step vs 126 MB L2)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_cell": bpc},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": field_bytes / args.steps,
+                "d2h_bytes_per_step": field_bytes / args.steps + 12,
+                "note": "input field uploaded from pinned host memory and final field downloaded inside the "
+                        "timed region; per-step mass/health read back; through LBM_Solver3D.step"},
+        "gpu_launches": args.steps,
+        "health_nonfinite_cells": health,
+    }
+    c = clk.summary()
+    if c is not None:
+        out["clocks"] = c
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(n, budget_s=args.cpu_budget)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--storage", default="float32", choices=list(BYTES_PER_CELL))
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1 and args.impl == "reference" and rank != 0:
+        return  # the CPU arm runs on rank 0 only
+    if world > 1 and args.impl != "reference":
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group(backend="nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    try:
+        if args.impl == "reference":
+            out = run_reference(args, rank, world)
+        else:
+            out = run_ours(args, rank, world, dist)
+        if rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

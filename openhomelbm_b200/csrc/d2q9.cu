@@ -1,0 +1,649 @@
+// D2Q9 HOME-LBM step for sm_100a (replaces envs/lbm/lbm_func.py's kernels).
+//
+// One step of one or more worlds is four launches, the order of LBM_Solver.step
+// (envs/lbm/lbm_solver.py:104-141):
+//   1. prologue   precompute_transformed_segments (509-542), zeroing of the per-solid loads
+//                 (init_force, 503-506) and the bounding box of the cells near any solid;
+//   2. stream     stream_and_collide (322-467) for every fluid cell as if no solid existed;
+//   3. band       the cells near a solid (get_cutcell's own test, 567-576) are recomputed
+//                 with their cut links: the wall-velocity reconstruction of the link, the
+//                 momentum exchange and the torque (349-401); loads are summed in binary64;
+//   4. boundary   apply_bc (610-682) in the reference's sequential thread order, and the
+//                 binary32 copies of the loads (solid_forcex, solid_forcey, torque).
+// Cells in the band are computed twice; the band is a small part of the domain.
+
+#include <cmath>
+
+#include "hl_common.cuh"
+
+namespace hl {
+namespace d2 {
+
+// D2Q9 velocities and opposites in the reference's order (envs/lbm/lbm_core.py:128-130).
+__host__ __device__ constexpr int cx_of(int i) { return (i == 1 || i == 5 || i == 8) ? 1 : (i == 2 || i == 6 || i == 7) ? -1 : 0; }
+__host__ __device__ constexpr int cy_of(int i) { return (i == 3 || i == 5 || i == 6) ? 1 : (i == 4 || i == 7 || i == 8) ? -1 : 0; }
+__host__ __device__ constexpr int inv_of(int i) {
+  return i == 0 ? 0 : i == 1 ? 2 : i == 2 ? 1 : i == 3 ? 4 : i == 4 ? 3 : i == 5 ? 7 : i == 6 ? 8 : i == 7 ? 5 : 6;
+}
+constexpr int MAX_SOLIDS = 64;
+
+// mlCalDistribution (envs/lbm/lbm_func.py:685-788): population i rebuilt from (rho, u, S)
+// with the third-order Hermite terms Axxy, Axyy.
+template <class R> __device__ __forceinline__ R feq(const Mom2<R>& m, int i) {
+  const R Axxy = m.sxx * m.uy + R(2) * m.sxy * m.ux - R(2) * m.ux * m.ux * m.uy;
+  const R Axyy = m.syy * m.ux + R(2) * m.sxy * m.uy - R(2) * m.ux * m.uy * m.uy;
+  const R h = R(1.5);
+  switch (i) {
+    case 0: return R(4.0 / 9.0) * m.rho * (R(1) - h * m.sxx - h * m.syy);
+    case 1: return R(1.0 / 9.0) * m.rho * (R(1) + R(3) * m.ux + R(3) * m.sxx - h * m.syy - R(4.5) * Axyy);
+    case 2: return R(1.0 / 9.0) * m.rho * (R(1) - R(3) * m.ux + R(3) * m.sxx - h * m.syy + R(4.5) * Axyy);
+    case 3: return R(1.0 / 9.0) * m.rho * (R(1) + R(3) * m.uy - h * m.sxx + R(3) * m.syy - R(4.5) * Axxy);
+    case 4: return R(1.0 / 9.0) * m.rho * (R(1) - R(3) * m.uy - h * m.sxx + R(3) * m.syy + R(4.5) * Axxy);
+    case 5:
+      return R(1.0 / 36.0) * m.rho *
+             (R(1) + R(3) * (m.ux + m.uy) + R(3) * (m.sxx + m.syy + R(3) * m.sxy) + R(9) * (Axyy + Axxy));
+    case 6:
+      return R(1.0 / 36.0) * m.rho *
+             (R(1) - R(3) * m.ux + R(3) * m.uy + R(3) * (m.sxx + m.syy - R(3) * m.sxy) + R(9) * (Axxy - Axyy));
+    case 7:
+      return R(1.0 / 36.0) * m.rho *
+             (R(1) - R(3) * m.ux - R(3) * m.uy + R(3) * (m.sxx + m.syy + R(3) * m.sxy) - R(9) * (Axxy + Axyy));
+    default:
+      return R(1.0 / 36.0) * m.rho *
+             (R(1) + R(3) * m.ux - R(3) * m.uy + R(3) * (m.sxx + m.syy - R(3) * m.sxy) - R(9) * (Axxy - Axyy));
+  }
+}
+
+// Moment-space collision of stream_and_collide (envs/lbm/lbm_func.py:414-467).
+template <class R> __device__ __forceinline__ Mom2<R> collide(const R pop[9], R Fx, R Fy, R omega) {
+  const R rho = pop[0] + pop[1] + pop[2] + pop[3] + pop[4] + pop[5] + pop[6] + pop[7] + pop[8];
+  const R inv = R(1) / rho;
+  const R ux = (pop[1] - pop[2] + pop[5] - pop[6] - pop[7] + pop[8] + R(0.5) * Fx) * inv;
+  const R uy = (pop[3] - pop[4] + pop[5] + pop[6] - pop[7] - pop[8] + R(0.5) * Fy) * inv;
+  const R pixx0 = pop[1] + pop[2] + pop[5] + pop[6] + pop[7] + pop[8];
+  const R piyy0 = pop[3] + pop[4] + pop[5] + pop[6] + pop[7] + pop[8];
+  const R pixy0 = pop[5] + pop[7] - pop[6] - pop[8];
+  const R Ru2 = rho * ux * ux, Rv2 = rho * uy * uy;
+  const R pxx_part = (pixx0 - piyy0) * R(0.5), pyy_part = (piyy0 - pixx0) * R(0.5);
+  const R o1 = R(1) - omega, oh = (R(1) + omega) * R(0.5), om = o1 * R(0.5);
+  const R pixy = o1 * pixy0 + ux * uy * rho * omega + (R(1) - R(0.5) * omega) * (Fy * ux + Fx * uy);
+  const R pixx = rho * R(1.0 / 3.0) + pxx_part * o1 + oh * Ru2 + om * Rv2 + Fx * ux + om * (Fx * ux - Fy * uy);
+  const R piyy = rho * R(1.0 / 3.0) + pyy_part * o1 + oh * Rv2 + om * Ru2 + Fy * uy + om * (Fy * uy - Fx * ux);
+  Mom2<R> m;
+  m.rho = rho;
+  m.ux = ux + Fx * inv * R(0.5);
+  m.uy = uy + Fy * inv * R(0.5);
+  m.sxx = pixx * inv - R(1.0 / 3.0);
+  m.syy = piyy * inv - R(1.0 / 3.0);
+  m.sxy = pixy * inv;
+  return m;
+}
+
+// One world of a (possibly batched) 2D launch.
+struct World {
+  void* buf[2];  // the two moment buffers; cur = buf[parity], post = buf[parity ^ 1]
+  const int* flag;
+  const float* fx;
+  const float* fy;
+  int nx, ny;
+  int periodic;
+  float omega, grid_length, time_step;
+  Scale sc;
+  int bc_type[4];
+  float bc_value[4][2];
+  // solids
+  int n_objects, max_segments;
+  const float* line;
+  const int* line_num;
+  float* tf;
+  float* tf_last;
+  const float* position;
+  const float* angle;
+  const float* scale;
+  const float* mass_center;
+  const float* max_radius;
+  double* loads64;
+  float* force_x;
+  float* force_y;
+  float* torque;
+  int* box;  // [4] x0, x1, y0, y1 of the cells near a solid (inclusive), empty if x0 > x1
+};
+
+// Kernel argument: one world by value, or a device array of worlds (batched launches).
+struct Launch {
+  World one;
+  const World* many;
+  int parity;
+};
+
+__device__ __forceinline__ const World& world_of(const Launch& L, int k) { return L.many ? L.many[k] : L.one; }
+__device__ __forceinline__ const void* cur_of(const Launch& L, const World& w) { return w.buf[L.parity]; }
+__device__ __forceinline__ void* post_of(const Launch& L, const World& w) { return w.buf[L.parity ^ 1]; }
+
+template <class S> __device__ __forceinline__ Mom2<typename S::R> load2(const World& w, long long N, long long i,
+                                                                        const typename S::T* m) {
+  typename S::R raw[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) raw[k] = S::to_r(m[k * N + i]);
+  return decode2<S>(raw, w.sc);
+}
+template <class S> __device__ __forceinline__ void store2(const World& w, long long N, long long i, typename S::T* m,
+                                                          const Mom2<typename S::R>& v) {
+  typename S::R raw[6];
+  encode2<S>(v, w.sc, raw);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) m[k * N + i] = S::from_r(raw[k]);
+}
+
+__device__ __forceinline__ bool is_fluid(const World& w, int x, int y, long long i) {
+  if (w.flag) return w.flag[i] == ML_FLUID;
+  if (w.periodic) return true;
+  return x > 0 && x < w.nx - 1 && y > 0 && y < w.ny - 1;
+}
+
+// -------------------------------------------------------------------------- 1. prologue
+__global__ void prologue_kernel(const __grid_constant__ Launch L) {
+  const World& w = world_of(L, blockIdx.x);
+  __shared__ int box[4];
+  if (threadIdx.x == 0) {
+    box[0] = w.nx;
+    box[1] = -1;
+    box[2] = w.ny;
+    box[3] = -1;
+  }
+  __syncthreads();
+  const int total = w.n_objects * w.max_segments;
+  for (int k = threadIdx.x; k < total; k += blockDim.x) {
+    const int sid = k / w.max_segments, idx = k % w.max_segments;
+    if (idx >= w.line_num[sid]) continue;
+    // precompute_transformed_segments, envs/lbm/lbm_func.py:509-542
+    const float scale = w.scale[sid] * float(w.nx);
+    float sa, ca;
+    sincosf(w.angle[sid], &sa, &ca);
+    const float ppx = (w.line[2 * k] - w.mass_center[2 * sid]) * scale;
+    const float ppy = (w.line[2 * k + 1] - w.mass_center[2 * sid + 1]) * scale;
+    const float nx_ = ppx * ca - ppy * sa + w.position[2 * sid];
+    const float ny_ = ppx * sa + ppy * ca + w.position[2 * sid + 1];
+    const float ox = w.tf[2 * k], oy = w.tf[2 * k + 1];
+    if (ox == 0.f && oy == 0.f) {
+      w.tf_last[2 * k] = nx_;
+      w.tf_last[2 * k + 1] = ny_;
+    } else {
+      w.tf_last[2 * k] = ox;
+      w.tf_last[2 * k + 1] = oy;
+    }
+    w.tf[2 * k] = nx_;
+    w.tf[2 * k + 1] = ny_;
+  }
+  for (int s = threadIdx.x; s < w.n_objects; s += blockDim.x) {
+    w.loads64[3 * s] = w.loads64[3 * s + 1] = w.loads64[3 * s + 2] = 0.0;
+    if (w.line_num[s] <= 0) continue;
+    // cells with |cell - position|^2 <= max_radius * (scale nx)^2 (get_cutcell, 567-576)
+    const float sc = w.scale[s] * float(w.nx);
+    const float r = sqrtf(fmaxf(w.max_radius[s] * sc * sc, 0.f)) + 1.f;
+    const float px = w.position[2 * s], py = w.position[2 * s + 1];
+    if (!(isfinite(px) && isfinite(py) && isfinite(r))) continue;
+    const int x0 = max(0, int(floorf(px - r))), x1 = min(w.nx - 1, int(ceilf(px + r)));
+    const int y0 = max(0, int(floorf(py - r))), y1 = min(w.ny - 1, int(ceilf(py + r)));
+    if (x0 > x1 || y0 > y1) continue;
+    atomicMin(&box[0], x0);
+    atomicMax(&box[1], x1);
+    atomicMin(&box[2], y0);
+    atomicMax(&box[3], y1);
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) w.box[threadIdx.x] = box[threadIdx.x];
+}
+
+// -------------------------------------------------------------------------- 2. stream
+// Pull streaming for every fluid cell, ignoring solids. blockIdx.z = world.
+template <class S> __global__ void __launch_bounds__(256) stream_kernel(const __grid_constant__ Launch L) {
+  using R = typename S::R;
+  using T = typename S::T;
+  const World& w = world_of(L, blockIdx.z);
+  const int y = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int x = blockIdx.y * 8 + (threadIdx.x >> 5);
+  if (x >= w.nx || y >= w.ny) return;
+  const long long N = (long long)w.nx * w.ny;
+  const long long c = (long long)x * w.ny + y;
+  if (!is_fluid(w, x, y, c)) return;
+  const T* cur = static_cast<const T*>(cur_of(L, w));
+  R pop[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    int xn = x - cx_of(i), yn = y - cy_of(i);
+    if (w.periodic) {
+      xn = wrap(xn, w.nx);
+      yn = wrap(yn, w.ny);
+    }
+    if (xn >= 0 && xn < w.nx && yn >= 0 && yn < w.ny) {
+      const Mom2<R> m = load2<S>(w, N, (long long)xn * w.ny + yn, cur);
+      pop[i] = fmax(feq<R>(m, i), R(0));
+    } else {
+      pop[i] = R(0);
+    }
+  }
+  const R Fx = w.fx ? R(w.fx[c]) : R(0), Fy = w.fy ? R(w.fy[c]) : R(0);
+  store2<S>(w, N, c, static_cast<T*>(post_of(L, w)), collide<R>(pop, Fx, Fy, R(w.omega)));
+}
+
+// -------------------------------------------------------------------------- 3. band
+struct Cut {
+  float t, ratio;
+  int solid, seg;
+};
+
+// get_cutcell (envs/lbm/lbm_func.py:545-607)
+__device__ Cut get_cutcell(const World& w, float x, float y, float dx, float dy) {
+  Cut r{-1.f, -1.f, -1, -1};
+  const float ax = x - dx, ay = y - dy, bx = x, by = y;
+  for (int s = 0; s < w.n_objects; ++s) {
+    const float px = x - w.position[2 * s], py = y - w.position[2 * s + 1];
+    const float scale = w.scale[s] * float(w.nx);
+    if (px * px + py * py > w.max_radius[s] * scale * scale) continue;
+    const int nseg = w.line_num[s];
+    const float* tf = w.tf + size_t(s) * w.max_segments * 2;
+    for (int n = 0; n < nseg; ++n) {
+      const int n1 = n + 1 == nseg ? 0 : n + 1;
+      const float cx = tf[2 * n], cy = tf[2 * n + 1], ex = tf[2 * n1], ey = tf[2 * n1 + 1];
+      const float abc = (ax - cx) * (by - cy) - (ay - cy) * (bx - cx);
+      const float abd = (ax - ex) * (by - ey) - (ay - ey) * (bx - ex);
+      if (abc * abd >= 0.f) continue;
+      const float cda = (cx - ax) * (ey - ay) - (cy - ay) * (ex - ax);
+      const float cdb = cda + abc - abd;
+      if (cda * cdb > 0.f) continue;
+      const float t = 1.f - cda / (abd - abc);
+      if (r.t < 0.f || t < r.t) {
+        r.t = t;
+        r.solid = s;
+        r.ratio = abc / (abc - abd);
+        r.seg = n;
+      }
+    }
+  }
+  return r;
+}
+
+template <class S> __global__ void __launch_bounds__(256) band_kernel(const __grid_constant__ Launch L) {
+  using R = typename S::R;
+  using T = typename S::T;
+  const World& w = world_of(L, blockIdx.y);
+  __shared__ double acc[MAX_SOLIDS * 3];
+  __shared__ int touched;
+  const int nsol = min(w.n_objects, MAX_SOLIDS);
+  for (int k = threadIdx.x; k < nsol * 3; k += blockDim.x) acc[k] = 0.0;
+  if (threadIdx.x == 0) touched = 0;
+  __syncthreads();
+  const int x0 = w.box[0], x1 = w.box[1], y0 = w.box[2], y1 = w.box[3];
+  const long long N = (long long)w.nx * w.ny;
+  const T* cur = static_cast<const T*>(cur_of(L, w));
+  if (x0 <= x1 && y0 <= y1) {
+    const int bw = y1 - y0 + 1;
+    const long long area = (long long)(x1 - x0 + 1) * bw;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < area;
+         k += (long long)gridDim.x * blockDim.x) {
+      const int x = x0 + int(k / bw), y = y0 + int(k % bw);
+      const long long c = (long long)x * w.ny + y;
+      if (!is_fluid(w, x, y, c)) continue;
+      bool near = false;
+      for (int s = 0; s < w.n_objects && !near; ++s) {
+        const float px = float(x) - w.position[2 * s], py = float(y) - w.position[2 * s + 1];
+        const float scale = w.scale[s] * float(w.nx);
+        near = w.line_num[s] > 0 && px * px + py * py <= w.max_radius[s] * scale * scale;
+      }
+      if (!near) continue;
+      const Mom2<R> me = load2<S>(w, N, c, cur);
+      R pop[9];
+      bool any_cut = false;
+#pragma unroll 1
+      for (int i = 0; i < 9; ++i) {
+        int xn = x - cx_of(i), yn = y - cy_of(i);
+        if (w.periodic) {
+          xn = wrap(xn, w.nx);
+          yn = wrap(yn, w.ny);
+        }
+        pop[i] = R(0);
+        if (!(xn >= 0 && xn < w.nx && yn >= 0 && yn < w.ny)) continue;
+        const Cut cc = get_cutcell(w, float(x), float(y), float(cx_of(i)), float(cy_of(i)));
+        if (cc.t >= 0.f && cc.solid >= 0) {
+          any_cut = true;
+          const int s = cc.solid, nseg = w.line_num[s];
+          const int n1 = cc.seg + 1 == nseg ? 0 : cc.seg + 1;
+          const float* tf = w.tf + size_t(s) * w.max_segments * 2;
+          const float* tl = w.tf_last + size_t(s) * w.max_segments * 2;
+          const float pcx = tf[2 * cc.seg] + (tf[2 * n1] - tf[2 * cc.seg]) * cc.ratio;
+          const float pcy = tf[2 * cc.seg + 1] + (tf[2 * n1 + 1] - tf[2 * cc.seg + 1]) * cc.ratio;
+          const float plx = tl[2 * cc.seg] + (tl[2 * n1] - tl[2 * cc.seg]) * cc.ratio;
+          const float ply = tl[2 * cc.seg + 1] + (tl[2 * n1 + 1] - tl[2 * cc.seg + 1]) * cc.ratio;
+          const R upx = R((pcx - plx) / w.time_step), upy = R((pcy - ply) / w.time_step);
+          const R rx = R(pcx - w.position[2 * s]), ry = R(pcy - w.position[2 * s + 1]);
+          Mom2<R> ms = me;
+          ms.ux = upx;
+          ms.uy = upy;
+          ms.sxx = upx * upx + me.sxx - me.ux * me.ux;
+          ms.syy = upy * upy + me.syy - me.uy * me.uy;
+          ms.sxy = upx * upy + me.sxy - me.ux * me.uy;
+          pop[i] = fmax(feq<R>(ms, i), R(0));
+          const int ii = inv_of(i);
+          const R cur_f = feq<R>(me, ii);
+          const R fx = cur_f * (R(cx_of(ii)) - upx) - pop[i] * (R(cx_of(i)) - upx);
+          const R fy = cur_f * (R(cy_of(ii)) - upy) - pop[i] * (R(cy_of(i)) - upy);
+          const R tq = (rx * fy - ry * fx) * R(w.grid_length);
+          if (s < MAX_SOLIDS) {
+            atomicAdd(&acc[3 * s], double(fx));
+            atomicAdd(&acc[3 * s + 1], double(fy));
+            atomicAdd(&acc[3 * s + 2], double(tq));
+            touched = 1;
+          }
+        } else {
+          pop[i] = fmax(feq<R>(load2<S>(w, N, (long long)xn * w.ny + yn, cur), i), R(0));
+        }
+      }
+      if (!any_cut) continue;  // the stream kernel's value is already this cell's update
+      const R Fx = w.fx ? R(w.fx[c]) : R(0), Fy = w.fy ? R(w.fy[c]) : R(0);
+      store2<S>(w, N, c, static_cast<T*>(post_of(L, w)), collide<R>(pop, Fx, Fy, R(w.omega)));
+    }
+  }
+  __syncthreads();
+  if (touched)
+    for (int k = threadIdx.x; k < nsol * 3; k += blockDim.x)
+      if (acc[k] != 0.0) atomicAdd(&w.loads64[k], acc[k]);
+}
+
+// -------------------------------------------------------------------------- 4. boundary
+// f_eq_home (envs/lbm/lbm_func.py:660-682): S of the clamped equilibrium populations.
+template <class R> __device__ void feq_s(R rho, R ux, R uy, R out[3]) {
+  const R usq = ux * ux + uy * uy;
+  R p[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const R w = i == 0 ? R(4.0 / 9.0) : i < 5 ? R(1.0 / 9.0) : R(1.0 / 36.0);
+    const R cu = R(cx_of(i)) * ux + R(cy_of(i)) * uy;
+    p[i] = fmax(rho * w * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq), R(0));
+  }
+  const R inv = R(1) / rho;
+  out[0] = (p[1] + p[2] + p[5] + p[6] + p[7] + p[8]) * inv - R(1.0 / 3.0);
+  out[1] = (p[3] + p[4] + p[5] + p[6] + p[7] + p[8]) * inv - R(1.0 / 3.0);
+  out[2] = (p[5] + p[7] - p[6] - p[8]) * inv;
+}
+
+// apply_bc_core (envs/lbm/lbm_func.py:634-657)
+template <class R> __device__ Mom2<R> bc_core(const World& w, int dr, const Mom2<R>& t, const Mom2<R>& nb) {
+  Mom2<R> r = t;
+  if (w.bc_type[dr] == 0) {
+    r.ux = R(w.bc_value[dr][0]);
+    r.uy = R(w.bc_value[dr][1]);
+  } else if (w.bc_type[dr] == 1) {
+    r.ux = nb.ux;
+    r.uy = nb.uy;
+  }
+  r.rho = nb.rho;
+  R sc[3], sb[3];
+  feq_s<R>(r.rho, r.ux, r.uy, sc);
+  feq_s<R>(nb.rho, nb.ux, nb.uy, sb);
+  r.sxx = sc[0] - sb[0] + nb.sxx;
+  r.syy = sc[1] - sb[1] + nb.syy;
+  r.sxy = sc[2] - sb[2] + nb.sxy;
+  return r;
+}
+
+// One CTA per world. Threads of the reference run in launch order (x outer, y inner): a
+// corner reads a neighbour on a low face (x = 0 or y = 0) before that neighbour's update
+// and one on a high face after it. Phase 1 updates the non-corner border cells, saving the
+// four cells corners read "before update"; phase 2 updates the corners.
+template <class S> __global__ void __launch_bounds__(512) boundary_kernel(const __grid_constant__ Launch L) {
+  using R = typename S::R;
+  using T = typename S::T;
+  const World& w = world_of(L, blockIdx.x);
+  const long long N = (long long)w.nx * w.ny;
+  T* post = static_cast<T*>(post_of(L, w));
+  __shared__ R snap[4][6];  // (1,0) (0,1) (1,ny-1) (nx-1,1)
+  if (!w.periodic) {
+    const int ex = w.nx - 2, ey = w.ny - 2;  // border cells per side without corners
+    const int total = 2 * ey + 2 * ex;
+    for (int k = threadIdx.x; k < total; k += blockDim.x) {
+      int x, y, dr, xn, yn;
+      if (k < ey) { x = 0; y = 1 + k; dr = 0; xn = 1; yn = y; }
+      else if (k < 2 * ey) { x = w.nx - 1; y = 1 + k - ey; dr = 2; xn = w.nx - 2; yn = y; }
+      else if (k < 2 * ey + ex) { x = 1 + k - 2 * ey; y = w.ny - 1; dr = 1; xn = x; yn = w.ny - 2; }
+      else { x = 1 + k - 2 * ey - ex; y = 0; dr = 3; xn = x; yn = 1; }
+      const long long c = (long long)x * w.ny + y;
+      const Mom2<R> t = load2<S>(w, N, c, post);
+      int slot = -1;
+      if (x == 1 && y == 0) slot = 0;
+      else if (x == 0 && y == 1) slot = 1;
+      else if (x == 1 && y == w.ny - 1) slot = 2;
+      else if (x == w.nx - 1 && y == 1) slot = 3;
+      if (slot >= 0) {
+        snap[slot][0] = t.rho; snap[slot][1] = t.ux; snap[slot][2] = t.uy;
+        snap[slot][3] = t.sxx; snap[slot][4] = t.syy; snap[slot][5] = t.sxy;
+      }
+      store2<S>(w, N, c, post, bc_core<R>(w, dr, t, load2<S>(w, N, (long long)xn * w.ny + yn, post)));
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      const int k = threadIdx.x;
+      const int x = (k & 2) ? w.nx - 1 : 0, y = (k & 1) ? w.ny - 1 : 0;
+      const long long c = (long long)x * w.ny + y;
+      Mom2<R> t = load2<S>(w, N, c, post);
+      auto from_snap = [&](int s) {
+        Mom2<R> m;
+        m.rho = snap[s][0]; m.ux = snap[s][1]; m.uy = snap[s][2];
+        m.sxx = snap[s][3]; m.syy = snap[s][4]; m.sxy = snap[s][5];
+        return m;
+      };
+      // x face first (left dr 0 / right dr 2), then y face (top dr 1 / bottom dr 3)
+      if (x == 0) t = bc_core<R>(w, 0, t, from_snap(y == 0 ? 0 : 2));
+      else t = bc_core<R>(w, 2, t, load2<S>(w, N, (long long)(w.nx - 2) * w.ny + y, post));
+      if (y == w.ny - 1) t = bc_core<R>(w, 1, t, load2<S>(w, N, (long long)x * w.ny + w.ny - 2, post));
+      else t = bc_core<R>(w, 3, t, x == 0 ? from_snap(1) : from_snap(3));
+      store2<S>(w, N, c, post, t);
+    }
+  }
+  for (int s = threadIdx.x; s < w.n_objects; s += blockDim.x) {
+    if (w.force_x) w.force_x[s] = float(w.loads64[3 * s]);
+    if (w.force_y) w.force_y[s] = float(w.loads64[3 * s + 1]);
+    if (w.torque) w.torque[s] = float(w.loads64[3 * s + 2]);
+  }
+}
+
+// -------------------------------------------------------------------------- init
+template <class S>
+__global__ void init_uniform_kernel(long long N, typename S::T* ma, typename S::T* mb, float* fx, float* fy, float ux,
+                                    float uy, Scale sc) {
+  using R = typename S::R;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  // InitFlow / set_uniform_flow_kernel (lbm_func.py:26-63, karman_lbm_env.py:15-53)
+  R p[9];
+  const R usq = R(ux) * R(ux) + R(uy) * R(uy);
+  for (int k = 0; k < 9; ++k) {
+    const R wk = k == 0 ? R(4.0 / 9.0) : k < 5 ? R(1.0 / 9.0) : R(1.0 / 36.0);
+    const R cu = R(cx_of(k)) * R(ux) + R(cy_of(k)) * R(uy);
+    p[k] = wk * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq);
+  }
+  const R pixx = p[1] + p[2] + p[5] + p[6] + p[7] + p[8];
+  const R piyy = p[3] + p[4] + p[5] + p[6] + p[7] + p[8];
+  const R pixy = p[5] + p[7] - p[6] - p[8];
+  Mom2<R> m;
+  m.rho = R(1);
+  m.ux = R(ux);
+  m.uy = R(uy);
+  m.sxx = pixx - pixx;  // cs2_local = pixx ("Very Important!!!", lbm_func.py:46)
+  m.syy = piyy - pixx;
+  m.sxy = pixy;
+  R raw[6];
+  encode2<S>(m, sc, raw);
+  for (int k = 0; k < 6; ++k) {
+    ma[k * N + i] = S::from_r(raw[k]);
+    mb[k * N + i] = S::from_r(raw[k]);
+  }
+  if (fx) fx[i] = 0.f;
+  if (fy) fy[i] = 0.f;
+}
+
+__global__ void init_boundary_kernel(int nx, int ny, int32_t* flag) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nx * ny) return;
+  const int x = int(i / ny), y = int(i % ny);
+  // InitBoundary (envs/lbm/lbm_func.py:17-23)
+  if (flag[i] != 1 && flag[i] != 6 && (x == 0 || x == nx - 1 || y == 0 || y == ny - 1)) flag[i] = ML_WALL;
+}
+
+}  // namespace d2
+}  // namespace hl
+
+// ============================================================================ C ABI
+using namespace hl;
+
+namespace {
+
+int fill_world(const hl_world2d* w, const hl_step2d* p, const hl_bc2d* bc, const hl_solids2d* s, d2::World* out) {
+  HL_CHECK_ARG(w != nullptr && p != nullptr, "d2q9: world or step parameters are NULL");
+  HL_CHECK_ARG(w->nx >= 3 && w->ny >= 3, "d2q9: grid must be at least 3 x 3 (got %d x %d)", w->nx, w->ny);
+  HL_CHECK_ARG(w->cur && w->post && w->cur != w->post, "d2q9: cur/post must be distinct device buffers");
+  HL_CHECK_ARG(p->vis_shear > 0.f, "d2q9: viscosity must be positive");
+  d2::World x{};
+  x.buf[0] = const_cast<void*>(w->cur);
+  x.buf[1] = w->post;
+  x.flag = w->flag;
+  x.fx = w->forcex;
+  x.fy = w->forcey;
+  x.nx = w->nx;
+  x.ny = w->ny;
+  x.periodic = w->periodic;
+  x.omega = 1.0f / (p->vis_shear * 3.0f + 0.5f);
+  x.grid_length = p->grid_length > 0.f ? p->grid_length : 1.0f / float(w->nx);
+  x.time_step = p->time_step > 0.f ? p->time_step : 1.0f;
+  x.sc = make_scale(w->storage);
+  for (int f = 0; f < 4; ++f) {
+    x.bc_type[f] = bc ? bc->bc_type[f] : 1;
+    x.bc_value[f][0] = bc ? bc->bc_value[f][0] : 0.f;
+    x.bc_value[f][1] = bc ? bc->bc_value[f][1] : 0.f;
+  }
+  if (s && s->n_objects > 0) {
+    HL_CHECK_ARG(s->n_objects <= d2::MAX_SOLIDS, "d2q9: at most %d solids per world", d2::MAX_SOLIDS);
+    HL_CHECK_ARG(s->max_segments > 0, "d2q9: max_segments must be positive");
+    HL_CHECK_ARG(s->line && s->line_num && s->line_tf && s->line_tf_last && s->position && s->angle && s->scale &&
+                     s->mass_center && s->max_radius && s->loads64 && s->band_box,
+                 "d2q9: incomplete solid description");
+    x.n_objects = s->n_objects;
+    x.max_segments = s->max_segments;
+    x.line = s->line;
+    x.line_num = s->line_num;
+    x.tf = s->line_tf;
+    x.tf_last = s->line_tf_last;
+    x.position = s->position;
+    x.angle = s->angle;
+    x.scale = s->scale;
+    x.mass_center = s->mass_center;
+    x.max_radius = s->max_radius;
+    x.loads64 = s->loads64;
+    x.force_x = s->force_x;
+    x.force_y = s->force_y;
+    x.torque = s->torque;
+    x.box = s->band_box;
+  }
+  *out = x;
+  return HL_OK;
+}
+
+template <class S> int run_phases(const d2::Launch& L, int n, int maxx, int maxy, bool any_solid, int phases,
+                                  cudaStream_t st) {
+  if ((phases & HL_PHASE_SEGMENTS) && any_solid) {
+    d2::prologue_kernel<<<n, 256, 0, st>>>(L);
+    HL_LAUNCH_CHECK("d2q9 precompute_transformed_segments");
+  }
+  if (phases & HL_PHASE_STREAM) {
+    dim3 grid((maxy + 31) / 32, (maxx + 7) / 8, n);
+    d2::stream_kernel<S><<<grid, 256, 0, st>>>(L);
+    HL_LAUNCH_CHECK("d2q9 stream_and_collide");
+    if (any_solid) {
+      d2::band_kernel<S><<<dim3(64, n), 256, 0, st>>>(L);
+      HL_LAUNCH_CHECK("d2q9 cut-cell band");
+    }
+  }
+  if (phases & HL_PHASE_BC) {
+    d2::boundary_kernel<S><<<n, 512, 0, st>>>(L);
+    HL_LAUNCH_CHECK("d2q9 apply_bc");
+  }
+  return HL_OK;
+}
+
+int dispatch(hl_dtype dt, const d2::Launch& L, int n, int maxx, int maxy, bool any_solid, int phases, cudaStream_t st) {
+  switch (dt) {
+    case HL_F32: return run_phases<StoreF32>(L, n, maxx, maxy, any_solid, phases, st);
+    case HL_F64: return run_phases<StoreF64>(L, n, maxx, maxy, any_solid, phases, st);
+    case HL_F16: return run_phases<StoreF16>(L, n, maxx, maxy, any_solid, phases, st);
+    case HL_BF16: return run_phases<StoreBF16>(L, n, maxx, maxy, any_solid, phases, st);
+  }
+  set_error("d2q9: bad dtype");
+  return HL_ERR_ARG;
+}
+
+}  // namespace
+
+extern "C" int hl_d2q9_step_phases(const hl_world2d* w, const hl_step2d* p, const hl_bc2d* bc,
+                                   const hl_solids2d* solids, int phases, hl_stream stream) {
+  d2::Launch L{};
+  const int rc = fill_world(w, p, bc, solids, &L.one);
+  if (rc != HL_OK) return rc;
+  L.many = nullptr;
+  L.parity = 0;
+  return dispatch(w->storage.dtype, L, 1, w->nx, w->ny, L.one.n_objects > 0, phases, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hl_d2q9_step(const hl_world2d* w, const hl_step2d* p, const hl_bc2d* bc, const hl_solids2d* solids,
+                            hl_stream stream) {
+  return hl_d2q9_step_phases(w, p, bc, solids, HL_PHASE_ALL, stream);
+}
+
+extern "C" size_t hl_d2q9_desc_bytes(void) { return sizeof(d2::World); }
+
+extern "C" int hl_d2q9_pack(const hl_world2d* w, const hl_step2d* p, const hl_bc2d* bc, const hl_solids2d* solids,
+                            void* desc_host) {
+  HL_CHECK_ARG(desc_host != nullptr, "d2q9: descriptor buffer is NULL");
+  return fill_world(w, p, bc, solids, static_cast<d2::World*>(desc_host));
+}
+
+extern "C" int hl_d2q9_step_batch(const void* desc_dev, int n_worlds, int parity, hl_dtype dtype, int max_nx,
+                                  int max_ny, int any_solid, int phases, hl_stream stream) {
+  HL_CHECK_ARG(desc_dev != nullptr && n_worlds > 0 && max_nx > 0 && max_ny > 0, "d2q9: bad batch arguments");
+  HL_CHECK_ARG(parity == 0 || parity == 1, "d2q9: parity must be 0 or 1");
+  d2::Launch L{};
+  L.many = static_cast<const d2::World*>(desc_dev);
+  L.parity = parity;
+  return dispatch(dtype, L, n_worlds, max_nx, max_ny, any_solid != 0, phases, static_cast<cudaStream_t>(stream));
+}
+
+template <class S>
+static int init_uniform_2d_t(int nx, int ny, hl_storage sto, void* a, void* b, float* fx, float* fy, float ux, float uy,
+                             cudaStream_t st) {
+  const long long N = (long long)nx * ny;
+  d2::init_uniform_kernel<S><<<unsigned((N + 255) / 256), 256, 0, st>>>(
+      N, static_cast<typename S::T*>(a), static_cast<typename S::T*>(b), fx, fy, ux, uy, make_scale(sto));
+  HL_LAUNCH_CHECK("d2q9 init_uniform");
+  return HL_OK;
+}
+
+extern "C" int hl_d2q9_init_uniform(int nx, int ny, hl_storage sto, void* a, void* b, float* fx, float* fy, float ux,
+                                    float uy, hl_stream stream) {
+  HL_CHECK_ARG(nx > 0 && ny > 0 && a && b, "init_uniform_2d: bad arguments");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  switch (sto.dtype) {
+    case HL_F32: return init_uniform_2d_t<StoreF32>(nx, ny, sto, a, b, fx, fy, ux, uy, st);
+    case HL_F64: return init_uniform_2d_t<StoreF64>(nx, ny, sto, a, b, fx, fy, ux, uy, st);
+    case HL_F16: return init_uniform_2d_t<StoreF16>(nx, ny, sto, a, b, fx, fy, ux, uy, st);
+    case HL_BF16: return init_uniform_2d_t<StoreBF16>(nx, ny, sto, a, b, fx, fy, ux, uy, st);
+  }
+  set_error("init_uniform_2d: bad dtype");
+  return HL_ERR_ARG;
+}
+
+extern "C" int hl_d2q9_init_boundary(int nx, int ny, int32_t* flag, hl_stream stream) {
+  HL_CHECK_ARG(nx > 0 && ny > 0 && flag, "init_boundary_2d: bad arguments");
+  const long long N = (long long)nx * ny;
+  d2::init_boundary_kernel<<<unsigned((N + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(nx, ny, flag);
+  HL_LAUNCH_CHECK("d2q9 init_boundary");
+  return HL_OK;
+}

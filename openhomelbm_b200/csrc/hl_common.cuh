@@ -1,0 +1,203 @@
+// Shared device helpers of libhomelbm: error reporting, moment storage codecs, async copies.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/homelbm.h"
+
+namespace hl {
+
+// ----------------------------------------------------------------------------- errors
+void set_error(const char* fmt, ...);
+int cuda_status(cudaError_t e, const char* what);
+
+#define HL_CHECK_ARG(cond, ...)       \
+  do {                                \
+    if (!(cond)) {                    \
+      ::hl::set_error(__VA_ARGS__);   \
+      return HL_ERR_ARG;              \
+    }                                 \
+  } while (0)
+
+#define HL_LAUNCH_CHECK(what)                                        \
+  do {                                                               \
+    cudaError_t e_ = cudaGetLastError();                             \
+    if (e_ != cudaSuccess) return ::hl::cuda_status(e_, what);       \
+  } while (0)
+
+// ----------------------------------------------------------------------------- lattice
+constexpr int ML_FLUID = 0;
+constexpr int ML_WALL = 2;
+constexpr float CS2 = 1.0f / 3.0f;
+
+// ----------------------------------------------------------------------------- storage
+// Decoded moments of one D3Q27 cell, binary32 (binary64 for the accuracy build).
+template <class R> struct Mom3 {
+  R rho, ux, uy, uz, sxx, syy, szz, sxy, sxz, syz;
+};
+template <class R> struct Mom2 {
+  R rho, ux, uy, sxx, syy, sxy;
+};
+
+struct Scale {
+  float u, inv_u, s, inv_s;
+};
+
+inline Scale make_scale(const hl_storage& st) {
+  Scale s;
+  s.u = st.u_scale > 0.f ? st.u_scale : 1.f;
+  s.s = st.s_scale > 0.f ? st.s_scale : 1.f;
+  s.inv_u = 1.f / s.u;
+  s.inv_s = 1.f / s.s;
+  return s;
+}
+
+// Storage codecs: StoreF32 / StoreF64 keep the moments as they are; StoreF16 / StoreBF16
+// hold rho - 1, u / u_scale and (S - u u) / s_scale.
+struct StoreF32 {
+  using T = float;
+  using R = float;
+  static constexpr bool kEncoded = false;
+  __device__ static float to_r(T v) { return v; }
+  __device__ static T from_r(float v) { return v; }
+};
+struct StoreF64 {
+  using T = double;
+  using R = double;
+  static constexpr bool kEncoded = false;
+  __device__ static double to_r(T v) { return v; }
+  __device__ static T from_r(double v) { return v; }
+};
+struct StoreF16 {
+  using T = __half;
+  using R = float;
+  static constexpr bool kEncoded = true;
+  __device__ static float to_r(T v) { return __half2float(v); }
+  __device__ static T from_r(float v) { return __float2half_rn(v); }
+};
+struct StoreBF16 {
+  using T = __nv_bfloat16;
+  using R = float;
+  static constexpr bool kEncoded = true;
+  __device__ static float to_r(T v) { return __bfloat162float(v); }
+  __device__ static T from_r(float v) { return __float2bfloat16_rn(v); }
+};
+
+// raw[10] in plane order -> physical moments
+template <class S>
+__device__ __forceinline__ Mom3<typename S::R> decode3(const typename S::R raw[10], const Scale& sc) {
+  using R = typename S::R;
+  Mom3<R> m;
+  if constexpr (S::kEncoded) {
+    m.rho = raw[0] + R(1);
+    m.ux = raw[1] * sc.u;
+    m.uy = raw[2] * sc.u;
+    m.uz = raw[3] * sc.u;
+    m.sxx = fmaf(raw[4], sc.s, m.ux * m.ux);
+    m.syy = fmaf(raw[5], sc.s, m.uy * m.uy);
+    m.szz = fmaf(raw[6], sc.s, m.uz * m.uz);
+    m.sxy = fmaf(raw[7], sc.s, m.ux * m.uy);
+    m.sxz = fmaf(raw[8], sc.s, m.ux * m.uz);
+    m.syz = fmaf(raw[9], sc.s, m.uy * m.uz);
+  } else {
+    m.rho = raw[0];
+    m.ux = raw[1];
+    m.uy = raw[2];
+    m.uz = raw[3];
+    m.sxx = raw[4];
+    m.syy = raw[5];
+    m.szz = raw[6];
+    m.sxy = raw[7];
+    m.sxz = raw[8];
+    m.syz = raw[9];
+  }
+  return m;
+}
+
+template <class S>
+__device__ __forceinline__ void encode3(const Mom3<typename S::R>& m, const Scale& sc, typename S::R raw[10]) {
+  using R = typename S::R;
+  if constexpr (S::kEncoded) {
+    raw[0] = m.rho - R(1);
+    raw[1] = m.ux * sc.inv_u;
+    raw[2] = m.uy * sc.inv_u;
+    raw[3] = m.uz * sc.inv_u;
+    raw[4] = (m.sxx - m.ux * m.ux) * sc.inv_s;
+    raw[5] = (m.syy - m.uy * m.uy) * sc.inv_s;
+    raw[6] = (m.szz - m.uz * m.uz) * sc.inv_s;
+    raw[7] = (m.sxy - m.ux * m.uy) * sc.inv_s;
+    raw[8] = (m.sxz - m.ux * m.uz) * sc.inv_s;
+    raw[9] = (m.syz - m.uy * m.uz) * sc.inv_s;
+  } else {
+    raw[0] = m.rho;
+    raw[1] = m.ux;
+    raw[2] = m.uy;
+    raw[3] = m.uz;
+    raw[4] = m.sxx;
+    raw[5] = m.syy;
+    raw[6] = m.szz;
+    raw[7] = m.sxy;
+    raw[8] = m.sxz;
+    raw[9] = m.syz;
+  }
+}
+
+template <class S>
+__device__ __forceinline__ Mom2<typename S::R> decode2(const typename S::R raw[6], const Scale& sc) {
+  using R = typename S::R;
+  Mom2<R> m;
+  if constexpr (S::kEncoded) {
+    m.rho = raw[0] + R(1);
+    m.ux = raw[1] * sc.u;
+    m.uy = raw[2] * sc.u;
+    m.sxx = fmaf(raw[3], sc.s, m.ux * m.ux);
+    m.syy = fmaf(raw[4], sc.s, m.uy * m.uy);
+    m.sxy = fmaf(raw[5], sc.s, m.ux * m.uy);
+  } else {
+    m.rho = raw[0];
+    m.ux = raw[1];
+    m.uy = raw[2];
+    m.sxx = raw[3];
+    m.syy = raw[4];
+    m.sxy = raw[5];
+  }
+  return m;
+}
+
+template <class S>
+__device__ __forceinline__ void encode2(const Mom2<typename S::R>& m, const Scale& sc, typename S::R raw[6]) {
+  using R = typename S::R;
+  if constexpr (S::kEncoded) {
+    raw[0] = m.rho - R(1);
+    raw[1] = m.ux * sc.inv_u;
+    raw[2] = m.uy * sc.inv_u;
+    raw[3] = (m.sxx - m.ux * m.ux) * sc.inv_s;
+    raw[4] = (m.syy - m.uy * m.uy) * sc.inv_s;
+    raw[5] = (m.sxy - m.ux * m.uy) * sc.inv_s;
+  } else {
+    raw[0] = m.rho;
+    raw[1] = m.ux;
+    raw[2] = m.uy;
+    raw[3] = m.sxx;
+    raw[4] = m.syy;
+    raw[5] = m.sxy;
+  }
+}
+
+// ----------------------------------------------------------------------------- async copy
+// 4-byte global -> shared asynchronous copy; src_bytes = 0 zero-fills the destination.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, int src_bytes) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+}  // namespace hl
