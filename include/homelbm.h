@@ -55,6 +55,13 @@ typedef void* hl_stream; /* a cudaStream_t */
 HL_API const char* hl_last_error(void);
 HL_API const char* hl_version(void);
 
+/* Process-wide tuning knobs (no reference counterpart; for benchmarking and tests):
+ *   "d3q27_kernel": 0 automatic, 1 the asynchronous-copy kernel, 2 the TMA-staged kernel
+ *   "d3q27_chunks": 0 automatic, k > 0 splits x into k chunks per tile column
+ *   "d3q27_stages": 0 automatic (4), 3..5 planes staged by the TMA kernel
+ * Returns HL_ERR_ARG for an unknown key. A CUDA graph keeps the choice it was captured with. */
+HL_API int hl_set_tuning(const char* key, int value);
+
 /* ------------------------------------------------------------------ encoding */
 /* Reduced-precision storage (HL_F16 / HL_BF16): a cell stores rho-1, u/u_scale and the
  * non-equilibrium second moment (S - u u)/s_scale; every kernel decodes to binary32 on load
@@ -100,9 +107,9 @@ typedef struct {
 /* Replaces stream_and_collide_3d (envs/lbm3d/lbm_func_3d.py:364-604) for worlds without
  * immersed solids: pull streaming from the neighbours' moments with the reference's
  * second-order reconstruction (mlCalEquilibrium3D_s, 224-251), clamped at zero, then the
- * regularised collision (564-604) with relaxation omega = 1/(3 vis_shear + 0.5).
- * diag may be NULL. */
-HL_API int hl_d3q27_stream_collide(const hl_world3d* w, float vis_shear, const hl_diag* diag,
+ * regularised collision (564-604) with relaxation omega = 1/(3 vis_shear + 0.5), evaluated
+ * in the storage precision (binary32, or binary64 for HL_F64). diag may be NULL. */
+HL_API int hl_d3q27_stream_collide(const hl_world3d* w, double vis_shear, const hl_diag* diag,
                             hl_stream stream);
 
 /* Replaces apply_bc_3d (envs/lbm3d/lbm_func_3d.py:607-624) on post, with the reference's
@@ -144,7 +151,7 @@ typedef struct {
 
 /* Scalar parameters of HomeFlow used by the step (lbm_core.py:103-135). */
 typedef struct {
-  float vis_shear;       /* kinematic viscosity; omega = 1/(3 vis_shear + 0.5) */
+  double vis_shear;      /* kinematic viscosity; omega = 1/(3 vis_shear + 0.5) in the storage precision */
   float grid_length;     /* torque scale, the reference's 1/nx; <= 0 selects 1/nx */
   float time_step;       /* wall velocity = displacement / time_step; <= 0 selects 1 */
 } hl_step2d;

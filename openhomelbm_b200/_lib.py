@@ -48,7 +48,7 @@ class hl_world2d(Structure):
 
 
 class hl_step2d(Structure):
-    _fields_ = [("vis_shear", c_float), ("grid_length", c_float), ("time_step", c_float)]
+    _fields_ = [("vis_shear", c_double), ("grid_length", c_float), ("time_step", c_float)]
 
 
 class hl_bc2d(Structure):
@@ -69,7 +69,8 @@ _lib = None
 _SIGS = {
     "hl_last_error": ([], c_char_p),
     "hl_version": ([], c_char_p),
-    "hl_d3q27_stream_collide": ([POINTER(hl_world3d), c_float, POINTER(hl_diag), c_void_p], c_int),
+    "hl_set_tuning": ([c_char_p, c_int], c_int),
+    "hl_d3q27_stream_collide": ([POINTER(hl_world3d), c_double, POINTER(hl_diag), c_void_p], c_int),
     "hl_d3q27_apply_bc": ([POINTER(hl_world3d), POINTER(hl_bc3d), c_void_p, c_void_p], c_int),
     "hl_d3q27_scratch_bytes": ([POINTER(hl_world3d)], c_size_t),
     "hl_d3q27_bc_scratch_bytes": ([POINTER(hl_world3d)], c_size_t),
@@ -159,3 +160,8 @@ def torch_dtype(code: int):
     import torch
 
     return {HL_F32: torch.float32, HL_F16: torch.float16, HL_BF16: torch.bfloat16, HL_F64: torch.float64}[code]
+
+
+def set_tuning(key: str, value: int) -> None:
+    """hl_set_tuning: process-wide kernel selection / work split knobs (see homelbm.h)."""
+    check(lib().hl_set_tuning(key.encode(), int(value)), "hl_set_tuning")

@@ -52,7 +52,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
     if force or _stale(LIB, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcuda"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs]
         subprocess.run(cmd, check=True)
     return LIB
 

@@ -27,36 +27,42 @@ __host__ __device__ constexpr int inv_of(int i) {
 }
 constexpr int MAX_SOLIDS = 64;
 
+// D2Q9 weight of direction i (lbm_core.py:127).
+template <class R> __device__ __forceinline__ R w2(int i) { return i == 0 ? R(4.0 / 9.0) : i < 5 ? R(1.0 / 9.0) : R(1.0 / 36.0); }
+
 // mlCalDistribution (envs/lbm/lbm_func.py:685-788): population i rebuilt from (rho, u, S)
-// with the third-order Hermite terms Axxy, Axyy.
-template <class R> __device__ __forceinline__ R feq(const Mom2<R>& m, int i) {
+// with the third-order Hermite terms Axxy, Axyy, returned as the deviation f_i - w_i
+// (the reference's bracket minus one: w_i (rho - 1 + rho (bracket_i - 1))).
+template <class R> __device__ __forceinline__ R feq_dev(const Mom2<R>& m, int i) {
   const R Axxy = m.sxx * m.uy + R(2) * m.sxy * m.ux - R(2) * m.ux * m.ux * m.uy;
   const R Axyy = m.syy * m.ux + R(2) * m.sxy * m.uy - R(2) * m.ux * m.uy * m.uy;
   const R h = R(1.5);
+  R b;
   switch (i) {
-    case 0: return R(4.0 / 9.0) * m.rho * (R(1) - h * m.sxx - h * m.syy);
-    case 1: return R(1.0 / 9.0) * m.rho * (R(1) + R(3) * m.ux + R(3) * m.sxx - h * m.syy - R(4.5) * Axyy);
-    case 2: return R(1.0 / 9.0) * m.rho * (R(1) - R(3) * m.ux + R(3) * m.sxx - h * m.syy + R(4.5) * Axyy);
-    case 3: return R(1.0 / 9.0) * m.rho * (R(1) + R(3) * m.uy - h * m.sxx + R(3) * m.syy - R(4.5) * Axxy);
-    case 4: return R(1.0 / 9.0) * m.rho * (R(1) - R(3) * m.uy - h * m.sxx + R(3) * m.syy + R(4.5) * Axxy);
-    case 5:
-      return R(1.0 / 36.0) * m.rho *
-             (R(1) + R(3) * (m.ux + m.uy) + R(3) * (m.sxx + m.syy + R(3) * m.sxy) + R(9) * (Axyy + Axxy));
-    case 6:
-      return R(1.0 / 36.0) * m.rho *
-             (R(1) - R(3) * m.ux + R(3) * m.uy + R(3) * (m.sxx + m.syy - R(3) * m.sxy) + R(9) * (Axxy - Axyy));
-    case 7:
-      return R(1.0 / 36.0) * m.rho *
-             (R(1) - R(3) * m.ux - R(3) * m.uy + R(3) * (m.sxx + m.syy + R(3) * m.sxy) - R(9) * (Axxy + Axyy));
-    default:
-      return R(1.0 / 36.0) * m.rho *
-             (R(1) + R(3) * m.ux - R(3) * m.uy + R(3) * (m.sxx + m.syy - R(3) * m.sxy) - R(9) * (Axxy - Axyy));
+    case 0: b = -h * m.sxx - h * m.syy; break;
+    case 1: b = R(3) * m.ux + R(3) * m.sxx - h * m.syy - R(4.5) * Axyy; break;
+    case 2: b = -R(3) * m.ux + R(3) * m.sxx - h * m.syy + R(4.5) * Axyy; break;
+    case 3: b = R(3) * m.uy - h * m.sxx + R(3) * m.syy - R(4.5) * Axxy; break;
+    case 4: b = -R(3) * m.uy - h * m.sxx + R(3) * m.syy + R(4.5) * Axxy; break;
+    case 5: b = R(3) * (m.ux + m.uy) + R(3) * (m.sxx + m.syy + R(3) * m.sxy) + R(9) * (Axyy + Axxy); break;
+    case 6: b = -R(3) * m.ux + R(3) * m.uy + R(3) * (m.sxx + m.syy - R(3) * m.sxy) + R(9) * (Axxy - Axyy); break;
+    case 7: b = -R(3) * m.ux - R(3) * m.uy + R(3) * (m.sxx + m.syy + R(3) * m.sxy) - R(9) * (Axxy + Axyy); break;
+    default: b = R(3) * m.ux - R(3) * m.uy + R(3) * (m.sxx + m.syy - R(3) * m.sxy) - R(9) * (Axxy - Axyy); break;
   }
+  return w2<R>(i) * (m.drho + m.rho * b);
 }
 
-// Moment-space collision of stream_and_collide (envs/lbm/lbm_func.py:414-467).
+// The clamped deviation: f_i >= 0 is f_i - w_i >= -w_i (lbm_func.py:411-412).
+template <class R> __device__ __forceinline__ R feq_dev_clamped(const Mom2<R>& m, int i) {
+  return fmax(feq_dev<R>(m, i), -w2<R>(i));
+}
+
+// Moment-space collision of stream_and_collide (envs/lbm/lbm_func.py:414-467) from deviation
+// populations pop[i] = f_i - w_i: rho = 1 + sum pop, Pi_aa = 1/3 + (deviation sum), and the
+// reference's S_aa = Pi_aa/rho - 1/3 equals X_aa / rho with no cancellation.
 template <class R> __device__ __forceinline__ Mom2<R> collide(const R pop[9], R Fx, R Fy, R omega) {
-  const R rho = pop[0] + pop[1] + pop[2] + pop[3] + pop[4] + pop[5] + pop[6] + pop[7] + pop[8];
+  const R drho = pop[0] + pop[1] + pop[2] + pop[3] + pop[4] + pop[5] + pop[6] + pop[7] + pop[8];
+  const R rho = R(1) + drho;
   const R inv = R(1) / rho;
   const R ux = (pop[1] - pop[2] + pop[5] - pop[6] - pop[7] + pop[8] + R(0.5) * Fx) * inv;
   const R uy = (pop[3] - pop[4] + pop[5] + pop[6] - pop[7] - pop[8] + R(0.5) * Fy) * inv;
@@ -67,17 +73,20 @@ template <class R> __device__ __forceinline__ Mom2<R> collide(const R pop[9], R 
   const R pxx_part = (pixx0 - piyy0) * R(0.5), pyy_part = (piyy0 - pixx0) * R(0.5);
   const R o1 = R(1) - omega, oh = (R(1) + omega) * R(0.5), om = o1 * R(0.5);
   const R pixy = o1 * pixy0 + ux * uy * rho * omega + (R(1) - R(0.5) * omega) * (Fy * ux + Fx * uy);
-  const R pixx = rho * R(1.0 / 3.0) + pxx_part * o1 + oh * Ru2 + om * Rv2 + Fx * ux + om * (Fx * ux - Fy * uy);
-  const R piyy = rho * R(1.0 / 3.0) + pyy_part * o1 + oh * Rv2 + om * Ru2 + Fy * uy + om * (Fy * uy - Fx * ux);
+  const R xxx = pxx_part * o1 + oh * Ru2 + om * Rv2 + Fx * ux + om * (Fx * ux - Fy * uy);
+  const R xyy = pyy_part * o1 + oh * Rv2 + om * Ru2 + Fy * uy + om * (Fy * uy - Fx * ux);
   Mom2<R> m;
   m.rho = rho;
+  m.drho = drho;
   m.ux = ux + Fx * inv * R(0.5);
   m.uy = uy + Fy * inv * R(0.5);
-  m.sxx = pixx * inv - R(1.0 / 3.0);
-  m.syy = piyy * inv - R(1.0 / 3.0);
+  m.sxx = xxx * inv;
+  m.syy = xyy * inv;
   m.sxy = pixy * inv;
   return m;
 }
+
+template <class R> __device__ __forceinline__ R omega_of(double vis) { return R(1) / (R(vis) * R(3) + R(0.5)); }
 
 // One world of a (possibly batched) 2D launch.
 struct World {
@@ -87,7 +96,8 @@ struct World {
   const float* fy;
   int nx, ny;
   int periodic;
-  float omega, grid_length, time_step;
+  double vis_shear;
+  float grid_length, time_step;
   Scale sc;
   int bc_type[4];
   float bc_value[4][2];
@@ -217,14 +227,13 @@ template <class S> __global__ void __launch_bounds__(256) stream_kernel(const __
       yn = wrap(yn, w.ny);
     }
     if (xn >= 0 && xn < w.nx && yn >= 0 && yn < w.ny) {
-      const Mom2<R> m = load2<S>(w, N, (long long)xn * w.ny + yn, cur);
-      pop[i] = fmax(feq<R>(m, i), R(0));
+      pop[i] = feq_dev_clamped<R>(load2<S>(w, N, (long long)xn * w.ny + yn, cur), i);
     } else {
-      pop[i] = R(0);
+      pop[i] = -w2<R>(i);  // out of range: f = 0
     }
   }
   const R Fx = w.fx ? R(w.fx[c]) : R(0), Fy = w.fy ? R(w.fy[c]) : R(0);
-  store2<S>(w, N, c, static_cast<T*>(post_of(L, w)), collide<R>(pop, Fx, Fy, R(w.omega)));
+  store2<S>(w, N, c, static_cast<T*>(post_of(L, w)), collide<R>(pop, Fx, Fy, omega_of<R>(w.vis_shear)));
 }
 
 // -------------------------------------------------------------------------- 3. band
@@ -302,7 +311,7 @@ template <class S> __global__ void __launch_bounds__(256) band_kernel(const __gr
           xn = wrap(xn, w.nx);
           yn = wrap(yn, w.ny);
         }
-        pop[i] = R(0);
+        pop[i] = -w2<R>(i);
         if (!(xn >= 0 && xn < w.nx && yn >= 0 && yn < w.ny)) continue;
         const Cut cc = get_cutcell(w, float(x), float(y), float(cx_of(i)), float(cy_of(i)));
         if (cc.t >= 0.f && cc.solid >= 0) {
@@ -323,11 +332,13 @@ template <class S> __global__ void __launch_bounds__(256) band_kernel(const __gr
           ms.sxx = upx * upx + me.sxx - me.ux * me.ux;
           ms.syy = upy * upy + me.syy - me.uy * me.uy;
           ms.sxy = upx * upy + me.sxy - me.ux * me.uy;
-          pop[i] = fmax(feq<R>(ms, i), R(0));
+          pop[i] = feq_dev_clamped<R>(ms, i);
           const int ii = inv_of(i);
-          const R cur_f = feq<R>(me, ii);
-          const R fx = cur_f * (R(cx_of(ii)) - upx) - pop[i] * (R(cx_of(i)) - upx);
-          const R fy = cur_f * (R(cy_of(ii)) - upy) - pop[i] * (R(cy_of(i)) - upy);
+          // momentum exchange with the full populations f = w + (f - w)
+          const R cur_f = w2<R>(ii) + feq_dev<R>(me, ii);
+          const R pop_f = w2<R>(i) + pop[i];
+          const R fx = cur_f * (R(cx_of(ii)) - upx) - pop_f * (R(cx_of(i)) - upx);
+          const R fy = cur_f * (R(cy_of(ii)) - upy) - pop_f * (R(cy_of(i)) - upy);
           const R tq = (rx * fy - ry * fx) * R(w.grid_length);
           if (s < MAX_SOLIDS) {
             atomicAdd(&acc[3 * s], double(fx));
@@ -336,12 +347,12 @@ template <class S> __global__ void __launch_bounds__(256) band_kernel(const __gr
             touched = 1;
           }
         } else {
-          pop[i] = fmax(feq<R>(load2<S>(w, N, (long long)xn * w.ny + yn, cur), i), R(0));
+          pop[i] = feq_dev_clamped<R>(load2<S>(w, N, (long long)xn * w.ny + yn, cur), i);
         }
       }
       if (!any_cut) continue;  // the stream kernel's value is already this cell's update
       const R Fx = w.fx ? R(w.fx[c]) : R(0), Fy = w.fy ? R(w.fy[c]) : R(0);
-      store2<S>(w, N, c, static_cast<T*>(post_of(L, w)), collide<R>(pop, Fx, Fy, R(w.omega)));
+      store2<S>(w, N, c, static_cast<T*>(post_of(L, w)), collide<R>(pop, Fx, Fy, omega_of<R>(w.vis_shear)));
     }
   }
   __syncthreads();
@@ -351,19 +362,20 @@ template <class S> __global__ void __launch_bounds__(256) band_kernel(const __gr
 }
 
 // -------------------------------------------------------------------------- 4. boundary
-// f_eq_home (envs/lbm/lbm_func.py:660-682): S of the clamped equilibrium populations.
-template <class R> __device__ void feq_s(R rho, R ux, R uy, R out[3]) {
+// f_eq_home (envs/lbm/lbm_func.py:660-682): S of the clamped equilibrium populations, from
+// deviations: S_aa = (sum of f - w over c_a != 0 - (rho - 1)/3) / rho.
+template <class R> __device__ void feq_s(R rho, R drho, R ux, R uy, R out[3]) {
   const R usq = ux * ux + uy * uy;
   R p[9];
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
-    const R w = i == 0 ? R(4.0 / 9.0) : i < 5 ? R(1.0 / 9.0) : R(1.0 / 36.0);
     const R cu = R(cx_of(i)) * ux + R(cy_of(i)) * uy;
-    p[i] = fmax(rho * w * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq), R(0));
+    p[i] = fmax(w2<R>(i) * (drho + rho * (R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq)), -w2<R>(i));
   }
   const R inv = R(1) / rho;
-  out[0] = (p[1] + p[2] + p[5] + p[6] + p[7] + p[8]) * inv - R(1.0 / 3.0);
-  out[1] = (p[3] + p[4] + p[5] + p[6] + p[7] + p[8]) * inv - R(1.0 / 3.0);
+  const R d3 = drho * R(1.0 / 3.0);
+  out[0] = ((p[1] + p[2] + p[5] + p[6] + p[7] + p[8]) - d3) * inv;
+  out[1] = ((p[3] + p[4] + p[5] + p[6] + p[7] + p[8]) - d3) * inv;
   out[2] = (p[5] + p[7] - p[6] - p[8]) * inv;
 }
 
@@ -378,9 +390,10 @@ template <class R> __device__ Mom2<R> bc_core(const World& w, int dr, const Mom2
     r.uy = nb.uy;
   }
   r.rho = nb.rho;
+  r.drho = nb.drho;
   R sc[3], sb[3];
-  feq_s<R>(r.rho, r.ux, r.uy, sc);
-  feq_s<R>(nb.rho, nb.ux, nb.uy, sb);
+  feq_s<R>(r.rho, r.drho, r.ux, r.uy, sc);
+  feq_s<R>(nb.rho, nb.drho, nb.ux, nb.uy, sb);
   r.sxx = sc[0] - sb[0] + nb.sxx;
   r.syy = sc[1] - sb[1] + nb.syy;
   r.sxy = sc[2] - sb[2] + nb.sxy;
@@ -397,7 +410,7 @@ template <class S> __global__ void __launch_bounds__(512) boundary_kernel(const 
   const World& w = world_of(L, blockIdx.x);
   const long long N = (long long)w.nx * w.ny;
   T* post = static_cast<T*>(post_of(L, w));
-  __shared__ R snap[4][6];  // (1,0) (0,1) (1,ny-1) (nx-1,1)
+  __shared__ R snap[4][7];  // (1,0) (0,1) (1,ny-1) (nx-1,1)
   if (!w.periodic) {
     const int ex = w.nx - 2, ey = w.ny - 2;  // border cells per side without corners
     const int total = 2 * ey + 2 * ex;
@@ -416,7 +429,7 @@ template <class S> __global__ void __launch_bounds__(512) boundary_kernel(const 
       else if (x == w.nx - 1 && y == 1) slot = 3;
       if (slot >= 0) {
         snap[slot][0] = t.rho; snap[slot][1] = t.ux; snap[slot][2] = t.uy;
-        snap[slot][3] = t.sxx; snap[slot][4] = t.syy; snap[slot][5] = t.sxy;
+        snap[slot][3] = t.sxx; snap[slot][4] = t.syy; snap[slot][5] = t.sxy; snap[slot][6] = t.drho;
       }
       store2<S>(w, N, c, post, bc_core<R>(w, dr, t, load2<S>(w, N, (long long)xn * w.ny + yn, post)));
     }
@@ -429,7 +442,7 @@ template <class S> __global__ void __launch_bounds__(512) boundary_kernel(const 
       auto from_snap = [&](int s) {
         Mom2<R> m;
         m.rho = snap[s][0]; m.ux = snap[s][1]; m.uy = snap[s][2];
-        m.sxx = snap[s][3]; m.syy = snap[s][4]; m.sxy = snap[s][5];
+        m.sxx = snap[s][3]; m.syy = snap[s][4]; m.sxy = snap[s][5]; m.drho = snap[s][6];
         return m;
       };
       // x face first (left dr 0 / right dr 2), then y face (top dr 1 / bottom dr 3)
@@ -467,6 +480,7 @@ __global__ void init_uniform_kernel(long long N, typename S::T* ma, typename S::
   const R pixy = p[5] + p[7] - p[6] - p[8];
   Mom2<R> m;
   m.rho = R(1);
+  m.drho = R(0);
   m.ux = R(ux);
   m.uy = R(uy);
   m.sxx = pixx - pixx;  // cs2_local = pixx ("Very Important!!!", lbm_func.py:46)
@@ -502,7 +516,7 @@ int fill_world(const hl_world2d* w, const hl_step2d* p, const hl_bc2d* bc, const
   HL_CHECK_ARG(w != nullptr && p != nullptr, "d2q9: world or step parameters are NULL");
   HL_CHECK_ARG(w->nx >= 3 && w->ny >= 3, "d2q9: grid must be at least 3 x 3 (got %d x %d)", w->nx, w->ny);
   HL_CHECK_ARG(w->cur && w->post && w->cur != w->post, "d2q9: cur/post must be distinct device buffers");
-  HL_CHECK_ARG(p->vis_shear > 0.f, "d2q9: viscosity must be positive");
+  HL_CHECK_ARG(p->vis_shear > 0.0, "d2q9: viscosity must be positive");
   d2::World x{};
   x.buf[0] = const_cast<void*>(w->cur);
   x.buf[1] = w->post;
@@ -512,7 +526,7 @@ int fill_world(const hl_world2d* w, const hl_step2d* p, const hl_bc2d* bc, const
   x.nx = w->nx;
   x.ny = w->ny;
   x.periodic = w->periodic;
-  x.omega = 1.0f / (p->vis_shear * 3.0f + 0.5f);
+  x.vis_shear = p->vis_shear;
   x.grid_length = p->grid_length > 0.f ? p->grid_length : 1.0f / float(w->nx);
   x.time_step = p->time_step > 0.f ? p->time_step : 1.0f;
   x.sc = make_scale(w->storage);

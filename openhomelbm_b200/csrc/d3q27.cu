@@ -23,12 +23,17 @@
 //    (same c_x) to partial moments and keeps running sums for the planes x-1, x, x+1; a plane
 //    is complete once the source plane after it has been posted, then it collides (the
 //    regularised collision of lines 564-604, same formulas) and is written out.
+// Populations are carried as deviations from the rest state, f - w (g - 1 in the bracket):
+// sums then have no O(1) offset, the zero clamp f >= 0 becomes f - w >= -w, and S comes
+// out of the collision without the Pi/rho - 1/3 cancellation. The arithmetic is the
+// reference's, evaluated with less rounding.
 // HBM traffic is one read and one write of the 10 moments per cell (80 B in binary32).
 // Halo reloads come from L2 because all CTAs march the same x range in step.
 
 #include <cstdio>
+#include <cstdlib>
 
-#include "hl_common.cuh"
+#include "d3q27_core.cuh"
 
 namespace hl {
 namespace d3 {
@@ -43,172 +48,6 @@ template <int TY> struct Tile {
   static constexpr int NDST = TY * TZ;
   static constexpr int THREADS = ((NSRC + 31) / 32) * 32;
 };
-
-struct StepArgs {
-  const void* cur;
-  void* post;
-  long long N;  // cells per field plane
-  int nx, ny, nz;
-  int tiles_y, tiles_z, n_tiles;
-  int chunk_len, n_items;
-  float omega;
-  const float* force;
-  const int* flag;
-  Scale sc;
-  double* partials;        // [gridDim.x] mass partials
-  int* bad_partials;       // [gridDim.x]
-  unsigned* counter;       // completion counter (returns to 0 after each launch)
-  double* mass;
-  int* health;
-};
-
-// Partial moments of one destination cell.
-template <class R> struct Acc {
-  R rho, jx, jy, jz, pxx, pyy, pzz, pxy, pxz, pyz;
-  __device__ void zero() { rho = jx = jy = jz = pxx = pyy = pzz = pxy = pxz = pyz = R(0); }
-};
-
-// Weight of a direction by its number of non-zero components (lbm_core_3d.py:24-31).
-template <class R> __device__ __forceinline__ R w3(int nnz) {
-  return nnz == 0 ? R(8.0 / 27.0) : nnz == 1 ? R(2.0 / 27.0) : nnz == 2 ? R(1.0 / 54.0) : R(1.0 / 216.0);
-}
-
-__host__ __device__ constexpr int dir_index(int cx, int cy, int cz) { return ((cx + 1) * 3 + (cy + 1)) * 3 + (cz + 1); }
-
-// The 27 clamped, weighted populations a source cell sends, f[dir_index(c)].
-template <class R> __device__ __forceinline__ void rebuild_all(const Mom3<R>& m, R f[27]) {
-  const R usq = m.ux * m.ux + m.uy * m.uy + m.uz * m.uz;
-  const R trS = m.sxx + m.syy + m.szz;
-  const R A = m.rho * (R(1) - R(1.5) * usq - R(0.5) * trS);
-  const R r3 = R(3) * m.rho, r15 = R(1.5) * m.rho, r45 = R(4.5) * m.rho, r9 = R(9) * m.rho;
-  const R Bx = r3 * m.ux, By = r3 * m.uy, Bz = r3 * m.uz;
-  const R Cxx = r45 * m.ux * m.ux + r15 * m.sxx;
-  const R Cyy = r45 * m.uy * m.uy + r15 * m.syy;
-  const R Czz = r45 * m.uz * m.uz + r15 * m.szz;
-  const R Dxy = r9 * m.ux * m.uy + r3 * m.sxy;
-  const R Dxz = r9 * m.ux * m.uz + r3 * m.sxz;
-  const R Dyz = r9 * m.uy * m.uz + r3 * m.syz;
-  // P(cy, cz) = g restricted to c_x = 0; Q(cy, cz) = the c_x-linear part.
-  R P[3][3], Q[3][3];
-  const R aY = A + Cyy, aZ = A + Czz, aYZ = aY + Czz;
-  P[1][1] = A;
-  P[2][1] = aY + By;
-  P[0][1] = aY - By;
-  P[1][2] = aZ + Bz;
-  P[1][0] = aZ - Bz;
-  const R s1 = By + Bz, s2 = By - Bz, bp = aYZ + Dyz, bm = aYZ - Dyz;
-  P[2][2] = bp + s1;
-  P[0][0] = bp - s1;
-  P[2][0] = bm + s2;
-  P[0][2] = bm - s2;
-  const R t1 = Dxy + Dxz, t2 = Dxy - Dxz;
-  Q[1][1] = Bx;
-  Q[2][1] = Bx + Dxy;
-  Q[0][1] = Bx - Dxy;
-  Q[1][2] = Bx + Dxz;
-  Q[1][0] = Bx - Dxz;
-  Q[2][2] = Bx + t1;
-  Q[0][0] = Bx - t1;
-  Q[2][0] = Bx + t2;
-  Q[0][2] = Bx - t2;
-#pragma unroll
-  for (int yi = 0; yi < 3; ++yi)
-#pragma unroll
-    for (int zi = 0; zi < 3; ++zi) {
-      const int nyz = (yi != 1) + (zi != 1);
-      const R p = P[yi][zi], pc = p + Cxx, q = Q[yi][zi];
-      f[(1 * 3 + yi) * 3 + zi] = w3<R>(nyz) * fmax(p, R(0));
-      f[(2 * 3 + yi) * 3 + zi] = w3<R>(nyz + 1) * fmax(pc + q, R(0));
-      f[(0 * 3 + yi) * 3 + zi] = w3<R>(nyz + 1) * fmax(pc - q, R(0));
-    }
-}
-
-// Regularised collision of stream_and_collide_3d (envs/lbm3d/lbm_func_3d.py:564-604).
-template <class R>
-__device__ __forceinline__ Mom3<R> collide(const Acc<R>& a, R Fx, R Fy, R Fz, R omega) {
-  const R third = R(1.0 / 3.0);
-  const R rho = a.rho;
-  const R inv = R(1) / rho;
-  const R ux = (a.jx + R(0.5) * Fx) * inv;
-  const R uy = (a.jy + R(0.5) * Fy) * inv;
-  const R uz = (a.jz + R(0.5) * Fz) * inv;
-  const R pxx_part = (R(2) * a.pxx - a.pyy - a.pzz) * third;
-  const R pyy_part = (R(2) * a.pyy - a.pxx - a.pzz) * third;
-  const R pzz_part = (R(2) * a.pzz - a.pxx - a.pyy) * third;
-  const R RU2 = rho * ux * ux, RV2 = rho * uy * uy, RW2 = rho * uz * uz;
-  const R RUVW2 = (RU2 + RV2 + RW2) * third;
-  const R o1 = R(1) - omega;
-  const R ot = omega * third;
-  const R pxx = rho * third + pxx_part * o1 + RUVW2 + R(2) * RU2 * ot - RV2 * ot - RW2 * ot + Fx * ux;
-  const R pyy = rho * third + pyy_part * o1 + RUVW2 - RU2 * ot + R(2) * RV2 * ot - RW2 * ot + Fy * uy;
-  const R pzz = rho * third + pzz_part * o1 + RUVW2 - RU2 * ot - RV2 * ot + R(2) * RW2 * ot + Fz * uz;
-  const R pxy = a.pxy * o1 + ux * uy * rho * omega + (Fy * ux + Fx * uy) * R(0.5);
-  const R pxz = a.pxz * o1 + ux * uz * rho * omega + (Fz * ux + Fx * uz) * R(0.5);
-  const R pyz = a.pyz * o1 + uy * uz * rho * omega + (Fz * uy + Fy * uz) * R(0.5);
-  Mom3<R> m;
-  m.rho = rho;
-  m.ux = ux + Fx * inv * R(0.5);
-  m.uy = uy + Fy * inv * R(0.5);
-  m.uz = uz + Fz * inv * R(0.5);
-  m.sxx = pxx * inv - third;
-  m.syy = pyy * inv - third;
-  m.szz = pzz * inv - third;
-  m.sxy = pxy * inv;
-  m.sxz = pxz * inv;
-  m.syz = pyz * inv;
-  return m;
-}
-
-// Adds the group of 9 populations with one c_x (sx = c_x) to a destination's sums.
-template <class R> __device__ __forceinline__ void accumulate_group(Acc<R>& a, const R p[3][3], int sx) {
-  R Ry[3], Cz[3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    Ry[i] = p[i][0] + p[i][1] + p[i][2];
-    Cz[i] = p[0][i] + p[1][i] + p[2][i];
-  }
-  const R M0 = Ry[0] + Ry[1] + Ry[2];
-  const R My = Ry[2] - Ry[0], Myy = Ry[2] + Ry[0];
-  const R Mz = Cz[2] - Cz[0], Mzz = Cz[2] + Cz[0];
-  const R Myz = (p[2][2] + p[0][0]) - (p[2][0] + p[0][2]);
-  a.rho += M0;
-  a.jy += My;
-  a.jz += Mz;
-  a.pyy += Myy;
-  a.pzz += Mzz;
-  a.pyz += Myz;
-  if (sx != 0) {
-    a.pxx += M0;
-    if (sx > 0) {
-      a.jx += M0;
-      a.pxy += My;
-      a.pxz += Mz;
-    } else {
-      a.jx -= M0;
-      a.pxy -= My;
-      a.pxz -= Mz;
-    }
-  }
-}
-
-template <class R> __device__ __forceinline__ bool healthy(const Mom3<R>& m) {
-  const R s = m.ux + m.uy + m.uz + m.sxx + m.syy + m.szz + m.sxy + m.sxz + m.syz;
-  return isfinite(m.rho) && isfinite(s) && m.rho > R(0);
-}
-
-// Block-wide sum (deterministic order) of a per-thread value; result valid in thread 0.
-template <class V> __device__ V block_sum(V v, V* red) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __syncthreads();
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  V s = V(0);
-  if (threadIdx.x == 0)
-    for (int i = 0; i < int(blockDim.x + 31) / 32; ++i) s += red[i];
-  return s;
-}
 
 template <int TY, class S, bool PERIODIC, bool FORCE, bool FLAGS, bool DIAG>
 __global__ void __launch_bounds__(Tile<TY>::THREADS, 1) step_kernel(const StepArgs a) {
@@ -229,9 +68,9 @@ __global__ void __launch_bounds__(Tile<TY>::THREADS, 1) step_kernel(const StepAr
   const long long plane = (long long)a.ny * a.nz;
   const T* cur = static_cast<const T*>(a.cur);
   T* post = static_cast<T*>(a.post);
-  const R omega = R(a.omega);
+  const R omega = R(1) / (R(a.vis_shear) * R(3) + R(0.5));
 
-  R mass = R(0);
+  double mass = 0.0;
   int bad = 0;
 
   for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
@@ -286,16 +125,20 @@ __global__ void __launch_bounds__(Tile<TY>::THREADS, 1) step_kernel(const StepAr
         bool in = src_in;
         if (!PERIODIC) in = in && xs >= 0 && xs < a.nx;
         R f[27];
+        Mom3<R> m;
         if (in) {
           const T* s = stage + ((it % NSTAGE) * 10) * TL::NSRC + tid;
           R raw[10];
 #pragma unroll
           for (int k = 0; k < 10; ++k) raw[k] = S::to_r(s[k * TL::NSRC]);
-          rebuild_all<R>(decode3<S>(raw, a.sc), f);
+          m = decode3<S>(raw, a.sc);
         } else {
-#pragma unroll
-          for (int d = 0; d < 27; ++d) f[d] = R(0);
+          // outside the domain: zero populations (f - w = -w), the reference's out-of-range rule
+          m.rho = R(0);
+          m.drho = R(-1);
+          m.ux = m.uy = m.uz = m.sxx = m.syy = m.szz = m.sxy = m.sxz = m.syz = R(0);
         }
+        rebuild_all<R>(m, f);
 #pragma unroll
         for (int d = 0; d < 27; ++d) mb[d * TL::NSRC + tid] = f[d];
       }
@@ -336,7 +179,7 @@ __global__ void __launch_bounds__(Tile<TY>::THREADS, 1) step_kernel(const StepAr
 #pragma unroll
             for (int k = 0; k < 10; ++k) post[k * N + c] = S::from_r(raw[k]);
             if (DIAG) {
-              mass += m.rho;
+              mass += double(m.rho);
               bad += healthy<R>(m) ? 0 : 1;
             }
           }
@@ -351,7 +194,7 @@ __global__ void __launch_bounds__(Tile<TY>::THREADS, 1) step_kernel(const StepAr
   if (DIAG) {
     __shared__ double red_d[32];
     __shared__ int red_i[32];
-    const double ms = block_sum<double>(double(mass), red_d);
+    const double ms = block_sum<double>(mass, red_d);
     const int bs = block_sum<int>(bad, red_i);
     __shared__ bool last;
     if (tid == 0) {
@@ -408,7 +251,9 @@ template <int TY> Plan make_plan(int nx, int ny, int nz) {
   const int sms = num_sms();
   double best = -1.0;
   int best_c = 1;
-  for (int c = 1; c <= 16 && c <= nx; ++c) {
+  const int forced = g_tune_d3_chunks;
+  for (int c = 1; c <= 64 && c <= nx; ++c) {
+    if (forced > 0 && c != forced) continue;
     const int len = (nx + c - 1) / c;
     const int items = p.n_tiles * ((nx + len - 1) / len);
     const int waves = (items + sms - 1) / sms;
@@ -427,8 +272,17 @@ template <int TY> Plan make_plan(int nx, int ny, int nz) {
 
 size_t diag_scratch_bytes() { return size_t(num_sms()) * (sizeof(double) + sizeof(int)) + 64; }
 
+void fill_diag(StepArgs& a, const hl_diag* diag) {
+  char* s = static_cast<char*>(diag->scratch);
+  a.counter = reinterpret_cast<unsigned*>(s);
+  a.partials = reinterpret_cast<double*>(s + 16);
+  a.bad_partials = reinterpret_cast<int*>(s + 16 + sizeof(double) * num_sms());
+  a.mass = diag->mass;
+  a.health = diag->health;
+}
+
 template <int TY, class S, bool PERIODIC, bool FORCE, bool FLAGS, bool DIAG>
-int launch_step(const hl_world3d* w, float vis_shear, const hl_diag* diag, cudaStream_t st) {
+int launch_step(const hl_world3d* w, double vis_shear, const hl_diag* diag, cudaStream_t st) {
   const Plan p = make_plan<TY>(w->nx, w->ny, w->nz);
   StepArgs a{};
   a.cur = w->cur;
@@ -442,18 +296,11 @@ int launch_step(const hl_world3d* w, float vis_shear, const hl_diag* diag, cudaS
   a.n_tiles = p.n_tiles;
   a.chunk_len = p.chunk_len;
   a.n_items = p.n_items;
-  a.omega = 1.0f / (vis_shear * 3.0f + 0.5f);
+  a.vis_shear = vis_shear;
   a.force = w->force;
   a.flag = w->flag;
   a.sc = make_scale(w->storage);
-  if (DIAG) {
-    char* s = static_cast<char*>(diag->scratch);
-    a.counter = reinterpret_cast<unsigned*>(s);
-    a.partials = reinterpret_cast<double*>(s + 16);
-    a.bad_partials = reinterpret_cast<int*>(s + 16 + sizeof(double) * num_sms());
-    a.mass = diag->mass;
-    a.health = diag->health;
-  }
+  if (DIAG) fill_diag(a, diag);
   const size_t smem = smem_bytes<TY, S>();
   auto kern = step_kernel<TY, S, PERIODIC, FORCE, FLAGS, DIAG>;
   static bool attr_set = false;
@@ -468,7 +315,7 @@ int launch_step(const hl_world3d* w, float vis_shear, const hl_diag* diag, cudaS
 }
 
 template <int TY, class S>
-int dispatch_step(const hl_world3d* w, float vis, const hl_diag* d, cudaStream_t st) {
+int dispatch_step(const hl_world3d* w, double vis, const hl_diag* d, cudaStream_t st) {
   const bool P = w->periodic != 0, F = w->force != nullptr, G = w->flag != nullptr && !P,
              D = d != nullptr && d->scratch != nullptr;
 #define HL_D3_CASE(p, f, g, dg) \
@@ -495,7 +342,7 @@ int dispatch_step(const hl_world3d* w, float vis, const hl_diag* d, cudaStream_t
 
 using namespace hl;
 
-extern "C" int hl_d3q27_stream_collide(const hl_world3d* w, float vis_shear, const hl_diag* diag,
+extern "C" int hl_d3q27_stream_collide(const hl_world3d* w, double vis_shear, const hl_diag* diag,
                                        hl_stream stream) {
   HL_CHECK_ARG(w != nullptr, "d3q27: world is NULL");
   HL_CHECK_ARG(w->nx >= 1 && w->ny >= 1 && w->nz >= 1, "d3q27: bad dims %d x %d x %d", w->nx, w->ny, w->nz);
@@ -505,6 +352,11 @@ extern "C" int hl_d3q27_stream_collide(const hl_world3d* w, float vis_shear, con
                "d3q27: diagnostics scratch too small (%zu < %zu)", diag ? diag->scratch_bytes : 0,
                d3::diag_scratch_bytes());
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (g_tune_d3_kernel == 2 && !d3::tma_eligible(w)) {
+    set_error("d3q27: the TMA kernel needs ny %% 16 == 0, nz %% 32 == 0 and a non-float64 storage");
+    return HL_ERR_UNSUPPORTED;
+  }
+  if (g_tune_d3_kernel != 1 && d3::tma_eligible(w)) return d3::launch_step_tma(w, vis_shear, diag, st);
   switch (w->storage.dtype) {
     case HL_F32: return d3::dispatch_step<16, StoreF32>(w, vis_shear, diag, st);
     case HL_F64: return d3::dispatch_step<8, StoreF64>(w, vis_shear, diag, st);

@@ -74,8 +74,9 @@ template <class S> __device__ __forceinline__ void store_cell(const BcArgs& a, l
 }
 
 // f_eq_home_3d (envs/lbm3d/lbm_func_3d.py:651-686): S of the unclamped second-order
-// equilibrium populations of (rho, u). out = xx, yy, zz, xy, xz, yz.
-template <class R> __device__ void feq_s(R rho, R ux, R uy, R uz, R out[6]) {
+// equilibrium populations of (rho, u), from deviations f - w (S_aa = (sum - (rho-1)/3)/rho).
+// out = xx, yy, zz, xy, xz, yz.
+template <class R> __device__ void feq_s(R rho, R drho, R ux, R uy, R uz, R out[6]) {
   const R usq = ux * ux + uy * uy + uz * uz;
   R pxx = 0, pyy = 0, pzz = 0, pxy = 0, pxz = 0, pyz = 0;
 #pragma unroll
@@ -87,7 +88,7 @@ template <class R> __device__ void feq_s(R rho, R ux, R uy, R uz, R out[6]) {
         const int nnz = (cx != 0) + (cy != 0) + (cz != 0);
         const R w = nnz == 0 ? R(8.0 / 27.0) : nnz == 1 ? R(2.0 / 27.0) : nnz == 2 ? R(1.0 / 54.0) : R(1.0 / 216.0);
         const R cu = R(cx) * ux + R(cy) * uy + R(cz) * uz;
-        const R f = w * rho * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq);
+        const R f = w * (drho + rho * (R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq));
         if (cx) pxx += f;
         if (cy) pyy += f;
         if (cz) pzz += f;
@@ -96,10 +97,10 @@ template <class R> __device__ void feq_s(R rho, R ux, R uy, R uz, R out[6]) {
         if (cy * cz) pyz += R(cy * cz) * f;
       }
   const R inv = R(1) / rho;
-  const R third = R(1.0 / 3.0);
-  out[0] = pxx * inv - third;
-  out[1] = pyy * inv - third;
-  out[2] = pzz * inv - third;
+  const R d3 = drho * R(1.0 / 3.0);
+  out[0] = (pxx - d3) * inv;
+  out[1] = (pyy - d3) * inv;
+  out[2] = (pzz - d3) * inv;
   out[3] = pxy * inv;
   out[4] = pxz * inv;
   out[5] = pyz * inv;
@@ -119,9 +120,10 @@ template <class R> __device__ Mom3<R> bc_core(const BcArgs& a, int dr, const Mom
     r.uz = nb.uz;
   }
   r.rho = nb.rho;
+  r.drho = nb.drho;
   R sc[6], sb[6];
-  feq_s<R>(r.rho, r.ux, r.uy, r.uz, sc);
-  feq_s<R>(nb.rho, nb.ux, nb.uy, nb.uz, sb);
+  feq_s<R>(r.rho, r.drho, r.ux, r.uy, r.uz, sc);
+  feq_s<R>(nb.rho, nb.drho, nb.ux, nb.uy, nb.uz, sb);
   r.sxx = sc[0] - sb[0] + nb.sxx;
   r.syy = sc[1] - sb[1] + nb.syy;
   r.szz = sc[2] - sb[2] + nb.szz;
@@ -276,12 +278,14 @@ __global__ void init_uniform_kernel(long long N, typename S::T* ma, typename S::
       }
   Mom3<R> m;
   m.rho = rho;
+  m.drho = R(0);
   m.ux = R(ux);
   m.uy = R(uy);
   m.uz = R(uz);
+  // cs2_local = pixx is subtracted from every diagonal (lbm_func_3d.py:55-61)
   m.sxx = pxx * (R(1) / rho) - pxx;
-  m.syy = pyy * (R(1) / rho) - pyy;
-  m.szz = pzz * (R(1) / rho) - pzz;
+  m.syy = pyy * (R(1) / rho) - pxx;
+  m.szz = pzz * (R(1) / rho) - pxx;
   m.sxy = pxy / rho;
   m.sxz = pxz / rho;
   m.syz = pyz / rho;
@@ -308,6 +312,7 @@ __global__ void init_tgv_kernel(int nx, int ny, int nz, typename S::T* ma, typen
   const double rho = 1.0 + 3.0 * (double(u0) * u0 / 16.0) * (cos(2 * X) + cos(2 * Y)) * (cos(2 * Z) + 2.0);
   Mom3<R> m;
   m.rho = R(rho);
+  m.drho = R(rho - 1.0);
   m.ux = R(ux);
   m.uy = R(uy);
   m.uz = R(0);

@@ -13,6 +13,9 @@ namespace hl {
 // ----------------------------------------------------------------------------- errors
 void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* what);
+extern int g_tune_d3_kernel;  // hl_set_tuning("d3q27_kernel")
+extern int g_tune_d3_chunks;  // hl_set_tuning("d3q27_chunks")
+extern int g_tune_d3_stages;  // hl_set_tuning("d3q27_stages")
 
 #define HL_CHECK_ARG(cond, ...)       \
   do {                                \
@@ -34,12 +37,14 @@ constexpr int ML_WALL = 2;
 constexpr float CS2 = 1.0f / 3.0f;
 
 // ----------------------------------------------------------------------------- storage
-// Decoded moments of one D3Q27 cell, binary32 (binary64 for the accuracy build).
+// Decoded moments of one cell, binary32 (binary64 for the accuracy build). drho = rho - 1
+// is carried beside rho: kernels work with deviations from the rest state (populations as
+// f - w), which removes the O(1) offset from every sum.
 template <class R> struct Mom3 {
-  R rho, ux, uy, uz, sxx, syy, szz, sxy, sxz, syz;
+  R rho, drho, ux, uy, uz, sxx, syy, szz, sxy, sxz, syz;
 };
 template <class R> struct Mom2 {
-  R rho, ux, uy, sxx, syy, sxy;
+  R rho, drho, ux, uy, sxx, syy, sxy;
 };
 
 struct Scale {
@@ -92,6 +97,7 @@ __device__ __forceinline__ Mom3<typename S::R> decode3(const typename S::R raw[1
   using R = typename S::R;
   Mom3<R> m;
   if constexpr (S::kEncoded) {
+    m.drho = raw[0];
     m.rho = raw[0] + R(1);
     m.ux = raw[1] * sc.u;
     m.uy = raw[2] * sc.u;
@@ -104,6 +110,7 @@ __device__ __forceinline__ Mom3<typename S::R> decode3(const typename S::R raw[1
     m.syz = fmaf(raw[9], sc.s, m.uy * m.uz);
   } else {
     m.rho = raw[0];
+    m.drho = raw[0] - R(1);  // exact for rho in [0.5, 2] (Sterbenz)
     m.ux = raw[1];
     m.uy = raw[2];
     m.uz = raw[3];
@@ -121,7 +128,7 @@ template <class S>
 __device__ __forceinline__ void encode3(const Mom3<typename S::R>& m, const Scale& sc, typename S::R raw[10]) {
   using R = typename S::R;
   if constexpr (S::kEncoded) {
-    raw[0] = m.rho - R(1);
+    raw[0] = m.drho;
     raw[1] = m.ux * sc.inv_u;
     raw[2] = m.uy * sc.inv_u;
     raw[3] = m.uz * sc.inv_u;
@@ -150,6 +157,7 @@ __device__ __forceinline__ Mom2<typename S::R> decode2(const typename S::R raw[6
   using R = typename S::R;
   Mom2<R> m;
   if constexpr (S::kEncoded) {
+    m.drho = raw[0];
     m.rho = raw[0] + R(1);
     m.ux = raw[1] * sc.u;
     m.uy = raw[2] * sc.u;
@@ -158,6 +166,7 @@ __device__ __forceinline__ Mom2<typename S::R> decode2(const typename S::R raw[6
     m.sxy = fmaf(raw[5], sc.s, m.ux * m.uy);
   } else {
     m.rho = raw[0];
+    m.drho = raw[0] - R(1);
     m.ux = raw[1];
     m.uy = raw[2];
     m.sxx = raw[3];
@@ -171,7 +180,7 @@ template <class S>
 __device__ __forceinline__ void encode2(const Mom2<typename S::R>& m, const Scale& sc, typename S::R raw[6]) {
   using R = typename S::R;
   if constexpr (S::kEncoded) {
-    raw[0] = m.rho - R(1);
+    raw[0] = m.drho;
     raw[1] = m.ux * sc.inv_u;
     raw[2] = m.uy * sc.inv_u;
     raw[3] = (m.sxx - m.ux * m.ux) * sc.inv_s;

@@ -198,3 +198,83 @@ def border_flags_3d(nx, ny, nz):
     f = np.zeros((nx, ny, nz), np.int32)
     f[0], f[-1], f[:, 0], f[:, -1], f[:, :, 0], f[:, :, -1] = 2, 2, 2, 2, 2, 2
     return f
+
+
+def moment_errors(got, ref):
+    """Per-field errors of D2Q9 (6 planes) or D3Q27 (10 planes) moments, each divided by the
+    scale of the quantity it stores:
+
+    * rho by max|rho|;
+    * every velocity component by the largest speed component of the field (max |u_a| over a);
+    * a diagonal S_aa by max|S_aa + 1/3|: the reference stores S_aa = Pi_aa/rho - 1/3 and that
+      subtraction leaves about one binary32 ulp of 1/3 (3e-8) of absolute noise in S_aa, so
+      S_aa is only defined to that precision relative to Pi_aa/rho;
+    * an off-diagonal S_ab by the largest off-diagonal magnitude of the field.
+    """
+    import numpy as np
+
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    nm = ref.shape[0]
+    if nm == 6:
+        vel, diag, off = [1, 2], [3, 4], [5]
+    elif nm == 10:
+        vel, diag, off = [1, 2, 3], [4, 5, 6], [7, 8, 9]
+    else:
+        raise ValueError(nm)
+    d = np.abs(got - ref)
+    out = np.zeros(nm)
+    out[0] = d[0].max() / np.abs(ref[0]).max()
+    us = max(np.abs(ref[vel]).max(), 1e-12)
+    for k in vel:
+        out[k] = d[k].max() / us
+    for k in diag:
+        out[k] = d[k].max() / np.abs(ref[k] + 1.0 / 3.0).max()
+    os_ = max(np.abs(ref[off]).max(), 1e-12)
+    for k in off:
+        out[k] = d[k].max() / os_
+    return out
+
+
+def rel_l2(got, ref):
+    """Relative L2 errors of the moment groups: rho, the velocity vector and the second-moment
+    tensor Pi/rho = S + I/3 (the quantity the reference's S is taken from)."""
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    nm = ref.shape[0]
+    nd = 2 if nm == 6 else 3
+    vel = slice(1, 1 + nd)
+    sec = slice(1 + nd, nm)
+    shift = np.zeros_like(ref[sec])
+    shift[:nd] = 1.0 / 3.0
+    return {
+        "rho": float(np.linalg.norm(got[0] - ref[0]) / np.linalg.norm(ref[0])),
+        "u": float(np.linalg.norm(got[vel] - ref[vel]) / max(np.linalg.norm(ref[vel]), 1e-300)),
+        "Pi": float(np.linalg.norm(got[sec] - ref[sec]) / np.linalg.norm(ref[sec] + shift)),
+    }
+
+
+def check_parity(got, ref32, ref64, tol=1e-5, factor=3.0, floor=1e-7):
+    """The parity criterion of the tests.
+
+    (a) relative L2 of rho, u and Pi/rho against the binary32 reference (the oracle, which is
+        bit-exact to the reference's kernels) within ``tol``;
+    (b) per field, the max error against the binary64 evaluation of the same algorithm no
+        larger than ``factor`` times the reference's own binary32 error (plus ``floor``): the
+        CUDA result is as accurate as the reference. One binary32-vs-binary64 comparison is a
+        noisy estimate of a noise floor (moving walls, for instance, take their velocity from
+        differences of binary32 absolute positions), hence the factor of 3.
+    Returns a description of the failures (empty when both hold).
+    """
+    msgs = []
+    l2 = rel_l2(got, ref32)
+    bad = {k: v for k, v in l2.items() if not v <= tol}
+    if bad:
+        msgs.append(f"relative L2 vs reference above {tol}: {bad}")
+    e_got = moment_errors(got, ref64)
+    e_ref = moment_errors(ref32, ref64)
+    over = np.nonzero(~(e_got <= factor * e_ref + floor))[0]
+    if len(over):
+        msgs.append("less accurate than the reference on planes " +
+                    ", ".join(f"{k}: {e_got[k]:.2e} > {factor}x{e_ref[k]:.2e}" for k in over))
+    return msgs

@@ -18,3 +18,11 @@ def load_golden(name):
 
     with np.load(os.path.join(GOLDEN, f"{name}.npz")) as z:
         return {k: z[k] for k in z.files}
+
+
+
+def moment_errors(got, ref):
+    """Per-field scaled errors (see oracle.oracle.moment_errors)."""
+    from oracle.oracle import moment_errors as me
+
+    return me(got, ref)

@@ -50,6 +50,10 @@ def import_reference(ref):
     pkg("refenvs.lbm", f"{ref}/envs/lbm")
     pkg("refenvs.lbm3d", f"{ref}/envs/lbm3d")
     pkg("refenvs.lbm.karman", f"{ref}/envs/lbm/karman")
+    pkg("refenvs.lbm3d.karman", f"{ref}/envs/lbm3d/karman")
+    stub3 = types.ModuleType("refenvs.lbm3d.lbm_fluid_env_3d")
+    stub3.LBMFluidEnv3D = object
+    sys.modules["refenvs.lbm3d.lbm_fluid_env_3d"] = stub3
     # the gym environment base class is not needed by the kernels; stand it in
     stub = types.ModuleType("refenvs.lbm.lbm_fluid_env")
     stub.LBMFluidEnv = object
@@ -63,6 +67,7 @@ def import_reference(ref):
     mods.core3 = importlib.import_module("refenvs.lbm3d.lbm_core_3d")
     mods.func3 = importlib.import_module("refenvs.lbm3d.lbm_func_3d")
     mods.couple3 = importlib.import_module("refenvs.lbm3d.lbm_fluid_env_3d_func")
+    mods.karman3 = importlib.import_module("refenvs.lbm3d.karman.karman_lbm_env_3d")
     return mods
 
 
@@ -73,9 +78,6 @@ def _moments2d(flow):
 
 
 def _set_moments2d(flow, m):
-    for cur, post in ((flow.rho, flow.rho_post), (flow.Sxx, flow.Sxx_post),
-                      (flow.Syy, flow.Syy_post), (flow.Sxy, flow.Sxy_post)):
-        pass
     flow.rho.np[...] = m[0]
     flow.u.np[..., 0] = m[1]
     flow.u.np[..., 1] = m[2]
@@ -379,6 +381,28 @@ def case_coupling(R, name, seed):
     print(f"{name}: ok")
 
 
+def case_init(R, name):
+    """The initial-state kernels: InitFlow(3D), set_uniform_flow(_3d)_kernel, InitBoundary."""
+    wp = R.wp
+    f2 = R.core2.HomeFlow()
+    f2.Initialize(7, 5, n_objects=1)
+    fw2 = wp.array([f2], dtype=R.core2.HomeFlow)
+    wp.launch(R.func2.InitBoundary, dim=(1, 7, 5), inputs=[fw2])
+    wp.launch(R.karman2.set_uniform_flow_kernel, dim=(1, 7, 5), inputs=[fw2, 0.07, -0.03])
+    f3 = R.core3.HomeFlow3D()
+    f3.Initialize(5, 4, 6, n_objects=1)
+    fw3 = wp.array([f3], dtype=R.core3.HomeFlow3D)
+    wp.launch(R.func3.InitBoundary3D, dim=(1, 5, 4, 6), inputs=[fw3])
+    wp.launch(R.karman3.set_uniform_flow_3d_kernel, dim=(1, 5, 4, 6), inputs=[fw3, 0.05, -0.02, 0.03])
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"),
+                        u2=np.array([0.07, -0.03], np.float32), moments2=_moments2d(f2),
+                        post2=np.stack([f2.rho_post.np, f2.u_post.np[..., 0], f2.u_post.np[..., 1],
+                                        f2.Sxx_post.np, f2.Syy_post.np, f2.Sxy_post.np]), flag2=f2.flag.np.copy(),
+                        u3=np.array([0.05, -0.02, 0.03], np.float32), moments3=_moments3d(f3),
+                        post3=_moments3d(f3, post=True), flag3=f3.flag.np.copy())
+    print(f"{name}: ok")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("HOMELBM_REFERENCE", "/root/reference"))
@@ -413,6 +437,7 @@ def main():
             mesh=dict(radius=2.6, position=(5.7, 5.2, 6.1), velocity=(0.05, 0.02, -0.03),
                       axis=(0.3, 1.0, 0.2), omega=0.05)),
         "coupling": lambda: case_coupling(R, "coupling", 31),
+        "init": lambda: case_init(R, "init"),
     }
     for k, fn in cases.items():
         if args.only and k not in args.only.split(","):
