@@ -9,9 +9,9 @@
  * Conventions
  *  - All pointers are device pointers unless the name ends in _host. The caller owns every
  *    buffer (fields live in PyTorch tensors); the library allocates nothing in step calls.
- *  - Every call takes the CUDA stream to run on, performs no host synchronisation and no
- *    allocation, and can be captured into a CUDA graph (calls that need host-side set-up
- *    say so).
+ *  - Every call takes the CUDA stream to run on and performs no host synchronisation and no
+ *    allocation. hl_d3q27_stream_collide, hl_d3q27_apply_bc, the hl_d2q9_step* calls and the
+ *    init calls can be captured into a CUDA graph.
  *  - Return value: HL_OK (0) or a negative hl_status. hl_last_error() gives a message.
  *    Nothing throws across the ABI.
  *
@@ -118,6 +118,30 @@ HL_API int hl_d3q27_stream_collide(const hl_world3d* w, double vis_shear, const 
 HL_API int hl_d3q27_apply_bc(const hl_world3d* w, const hl_bc3d* bc, void* scratch, hl_stream stream);
 
 HL_API size_t hl_d3q27_scratch_bytes(const hl_world3d* w);
+
+/* hl_d3q27_stream_collide with its diagnostics, for callers that cannot allocate device
+ * memory. No counterpart in the reference.
+ *
+ * Some callers cannot call cudaMalloc: a host that has handed the whole HBM budget to a
+ * caching allocator or to resident fluid domains (a serving loop admits domains against a
+ * fixed budget), a real-time control loop that must not take allocation latency, or a
+ * plugin whose host owns all device memory. This entry point needs no scratch from them:
+ * the per-CTA partial sums and the completion counter live in a 16 KiB file-scope device
+ * array of the library, which every GPU that loads the library keeps until the process exits.
+ *  - Computes what hl_d3q27_stream_collide computes with a non-NULL diag: post <- step(cur),
+ *    *mass (binary64 sum of rho over updated cells) and *health (count of updated cells with
+ *    non-finite moments or rho <= 0); mass and health may be NULL. Storage float32 or
+ *    float64 (other storages return HL_ERR_ARG); it always runs the general kernel, never
+ *    the TMA-staged one, so its results can differ from hl_d3q27_stream_collide in rounding.
+ *  - Limit: 16 + 12 bytes per CTA of scratch, i.e. devices with up to 1364 SMs (a B200 has
+ *    148); larger needs are rejected with HL_ERR_ARG.
+ *  - The first call on a device resolves the array's device address (cudaGetSymbolAddress,
+ *    with that device current); make that first call before any stream capture.
+ *  - Every call shares the one array and leaves its last contents there; each call clears the
+ *    counter it needs first (stream-ordered). Calls that overlap on the GPU (other streams,
+ *    other host threads) race on the array: serialise them. */
+HL_API int hl_d3q27_stream_collide_noalloc(const hl_world3d* w, double vis_shear, double* mass, int32_t* health,
+                                           hl_stream stream);
 HL_API size_t hl_d3q27_bc_scratch_bytes(const hl_world3d* w);
 
 /* Replaces InitFlow3D (envs/lbm3d/lbm_func_3d.py:22-83) and set_uniform_flow_3d_kernel

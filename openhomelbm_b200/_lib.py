@@ -73,6 +73,7 @@ _SIGS = {
     "hl_d3q27_stream_collide": ([POINTER(hl_world3d), c_double, POINTER(hl_diag), c_void_p], c_int),
     "hl_d3q27_apply_bc": ([POINTER(hl_world3d), POINTER(hl_bc3d), c_void_p, c_void_p], c_int),
     "hl_d3q27_scratch_bytes": ([POINTER(hl_world3d)], c_size_t),
+    "hl_d3q27_stream_collide_noalloc": ([POINTER(hl_world3d), c_double, c_void_p, c_void_p, c_void_p], c_int),
     "hl_d3q27_bc_scratch_bytes": ([POINTER(hl_world3d)], c_size_t),
     "hl_d3q27_init_uniform": ([c_int, c_int, c_int, hl_storage, c_void_p, c_void_p, c_void_p, c_float,
                                c_float, c_float, c_void_p], c_int),

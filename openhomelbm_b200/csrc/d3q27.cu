@@ -367,3 +367,72 @@ extern "C" int hl_d3q27_stream_collide(const hl_world3d* w, double vis_shear, co
 }
 
 extern "C" size_t hl_d3q27_scratch_bytes(const hl_world3d*) { return d3::diag_scratch_bytes(); }
+
+// ============================================================================ allocation-free
+// hl_d3q27_stream_collide_noalloc: the diagnostics-enabled stream-collide for callers that
+// cannot allocate device memory (see include/homelbm.h). Its scratch - the per-CTA partial
+// sums and the completion counter - lives in a file-scope device array instead of a
+// caller-provided buffer.
+#include <mutex>
+
+namespace hl {
+namespace d3 {
+
+constexpr size_t kNoAllocScratchBytes = 16384;  // 16 + 12 bytes per CTA: up to 1364 CTAs (one per SM)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch on the current device. The host-side symbol is only a
+// stand-in, so the address is resolved once per device with that device current.
+static int noalloc_scratch(void** out) {
+  static std::mutex mu;
+  static void* addr[128] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e, "hl_d3q27_stream_collide_noalloc: cudaGetDevice");
+  if (dev < 0 || dev >= 128) {
+    set_error("hl_d3q27_stream_collide_noalloc: device ordinal %d out of range", dev);
+    return HL_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (addr[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      return cuda_status(e == cudaSuccess ? cudaErrorInvalidSymbol : e,
+                         "hl_d3q27_stream_collide_noalloc: cudaGetSymbolAddress");
+    addr[dev] = p;
+  }
+  *out = addr[dev];
+  return HL_OK;
+}
+
+}  // namespace d3
+}  // namespace hl
+
+extern "C" int hl_d3q27_stream_collide_noalloc(const hl_world3d* w, double vis_shear, double* mass, int32_t* health,
+                                               hl_stream stream) {
+  HL_CHECK_ARG(w != nullptr, "d3q27 (no-alloc): world is NULL");
+  HL_CHECK_ARG(w->nx >= 1 && w->ny >= 1 && w->nz >= 1, "d3q27 (no-alloc): bad dims %d x %d x %d", w->nx, w->ny, w->nz);
+  HL_CHECK_ARG(w->cur != nullptr && w->post != nullptr && w->cur != w->post,
+               "d3q27 (no-alloc): cur/post must be distinct");
+  HL_CHECK_ARG(vis_shear > 0.0, "d3q27 (no-alloc): viscosity must be positive");
+  HL_CHECK_ARG(w->storage.dtype == HL_F32 || w->storage.dtype == HL_F64,
+               "d3q27 (no-alloc): storage must be float32 or float64");
+  const d3::Plan plan =
+      w->storage.dtype == HL_F32 ? d3::make_plan<16>(w->nx, w->ny, w->nz) : d3::make_plan<8>(w->nx, w->ny, w->nz);
+  const size_t need = 16 + size_t(d3::num_sms()) * (sizeof(double) + sizeof(int));
+  HL_CHECK_ARG(need <= d3::kNoAllocScratchBytes && size_t(plan.grid) <= size_t(d3::num_sms()),
+               "d3q27 (no-alloc): needs %zu bytes of scratch for %d SMs; the static scratch holds %zu", need,
+               d3::num_sms(), d3::kNoAllocScratchBytes);
+  void* scratch = nullptr;
+  int rc = d3::noalloc_scratch(&scratch);
+  if (rc != HL_OK) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // the completion counter must start at zero (a previous launch leaves it at zero; clear it
+  // anyway so that an interrupted launch cannot poison the next one)
+  cudaError_t e = cudaMemsetAsync(scratch, 0, 16, st);
+  if (e != cudaSuccess) return cuda_status(e, "hl_d3q27_stream_collide_noalloc: clear counter");
+  hl_diag d{scratch, d3::kNoAllocScratchBytes, mass, health};
+  return w->storage.dtype == HL_F32 ? d3::dispatch_step<16, StoreF32>(w, vis_shear, &d, st)
+                                    : d3::dispatch_step<8, StoreF64>(w, vis_shear, &d, st);
+}
