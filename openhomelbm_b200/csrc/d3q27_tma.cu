@@ -1,9 +1,9 @@
-// D3Q27 stream-collide with TMA-staged source planes (sm_100a).
+// D3Q27 stream-collide with TMA-staged source planes and paired-plane arithmetic (sm_100a).
 //
-// Same arithmetic and mailbox exchange as the fallback kernel in d3q27.cu (source-side
-// population rebuild, (direction, source) mailbox in shared memory, x-marching with three
-// planes of partial moments). What differs is how each source plane reaches shared memory:
-// one elected thread issues nine tensor-memory-access (TMA) box copies per plane,
+// Same algorithm as the fallback kernel in d3q27.cu (source-side population rebuild,
+// exchange through a shared-memory mailbox, x-marching columns). Two things differ.
+//
+// Staging: one elected thread issues nine tensor-memory-access (TMA) box copies per plane,
 //
 //              z0-WZ..z0-1   z0..z0+31   z0+32..z0+32+WZ-1
 //   y0-1       corner        y edge      corner
@@ -16,11 +16,16 @@
 // rebuilds to zero populations: the reference's out-of-range rule). Completion is tracked by
 // one mbarrier per stage with bounded waits. No multicast: every CTA loads its own boxes.
 //
-// Per plane: every thread rebuilds the 27 populations of one interior source cell (threads
-// 0..99 then the 9 or 3 populations a halo cell sends into the tile) into a shared-memory
-// mailbox indexed by (direction, source); after a block barrier every thread reads the 27
-// populations arriving at its destination cell, adds them to partial moments of the planes
-// x-1, x, x+1 and collides the completed plane. NS stages keep NS-1 planes in flight.
+// Pairs of planes: each thread owns one (y, z) column of the 16 x 32 tile and handles two
+// consecutive source planes per iteration. Every quantity is a pair (lane 0 plane s0, lane 1
+// plane s0 + 1), so each arithmetic instruction is a packed FADD2 / FMUL2 / FFMA2 serving two
+// cells, and the mailbox entries are 8-byte pairs. A thread rebuilds the 27 populations of
+// its cell pair, keeps the three with c_y = c_z = 0 in registers and writes the other 24 to
+// the mailbox slot of the destination cell (threads 0..99 add the 9 or 3 populations a halo
+// cell sends into the tile). After a block barrier each thread reads its 24 incoming pairs,
+// forms the sums of the c_x = -1, 0, +1 groups, and completes the destination planes s0 - 1
+// and s0 from them and from the previous pair's sums. Four stages keep the next pair in
+// flight while the current one is computed. Two barriers per pair: one per plane.
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -33,6 +38,7 @@
 #include <tuple>
 
 #include "d3q27_core.cuh"
+#include "d3q27_pair.cuh"
 
 namespace hl {
 namespace d3 {
@@ -64,9 +70,9 @@ template <class T, int NSTAGE> struct Geo {
   static constexpr int OFF_C = OFF_ZHI + B_ZE;
   static constexpr int STAGE_BYTES = OFF_C + 4 * B_C;
   static constexpr int TX_BYTES = 10 * int(sizeof(T)) * (E_MID + 2 * E_YE + 2 * E_ZE + 4 * E_C);
-  static constexpr int MB_BYTES = 27 * NSRC * 4;                      // the mailbox
+  static constexpr int MB_BYTES = 24 * NDST * 8;  // mailbox: 24 directions x 512 cells x 2 planes
   static constexpr int MB_OFF = NSTAGE * STAGE_BYTES;
-  static constexpr int BAR_OFF = MB_OFF + MB_BYTES;                   // mbarriers
+  static constexpr int BAR_OFF = MB_OFF + MB_BYTES;  // mbarriers
   static constexpr int SMEM = BAR_OFF + NSTAGE * 8 + 16 + 128;  // + alignment slack
 };
 
@@ -106,20 +112,123 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------- kernel
+// Mailbox slot of direction (xi, yi, zi) with (yi, zi) != (1, 1): the populations a
+// destination receives from a y/z neighbour, indexed by (direction, destination cell).
+__host__ __device__ constexpr int mb_dir(int xi, int yi, int zi) {
+  return xi * 8 + ((yi * 3 + zi) < 4 ? (yi * 3 + zi) : (yi * 3 + zi - 1));
+}
+
+// Sums of one direction group (fixed c_x) over its 9 populations p[yi][zi], for the pair
+// of source planes: the parts of rho, j_y, j_z, Pi_yy, Pi_zz, Pi_yz it contributes (and, for
+// c_x = -1 / +1, of rho * c_x, Pi_xx, Pi_xy, Pi_xz through its sign).
+struct GroupSums {
+  P2 m0, my, myy, mz, mzz, myz;
+};
+
+__device__ __forceinline__ GroupSums group_sums(const P2 p[3][3]) {
+  const P2 ry0 = p[0][0] + p[0][1] + p[0][2];
+  const P2 ry1 = p[1][0] + p[1][1] + p[1][2];
+  const P2 ry2 = p[2][0] + p[2][1] + p[2][2];
+  const P2 cz0 = p[0][0] + p[1][0] + p[2][0];
+  const P2 cz2 = p[0][2] + p[1][2] + p[2][2];
+  GroupSums g;
+  g.myy = ry2 + ry0;
+  g.my = ry2 - ry0;
+  g.m0 = g.myy + ry1;
+  g.mzz = cz2 + cz0;
+  g.mz = cz2 - cz0;
+  g.myz = (p[2][2] + p[0][0]) - (p[2][0] + p[0][2]);
+  return g;
+}
+
+// Raw stored planes of a cell pair -> physical moments (decode3 of hl_common.cuh, per lane).
+template <class S> __device__ __forceinline__ Mom3<P2> decode_pair(const P2 raw[10], const Scale& sc) {
+  Mom3<P2> m;
+  if constexpr (S::kEncoded) {
+    const P2 su(sc.u), ss(sc.s);
+    m.drho = raw[0];
+    m.rho = raw[0] + P2(1.0);
+    m.ux = raw[1] * su;
+    m.uy = raw[2] * su;
+    m.uz = raw[3] * su;
+    m.sxx = raw[4] * ss + m.ux * m.ux;
+    m.syy = raw[5] * ss + m.uy * m.uy;
+    m.szz = raw[6] * ss + m.uz * m.uz;
+    m.sxy = raw[7] * ss + m.ux * m.uy;
+    m.sxz = raw[8] * ss + m.ux * m.uz;
+    m.syz = raw[9] * ss + m.uy * m.uz;
+  } else {
+    m.rho = raw[0];
+    m.drho = raw[0] - P2(1.0);
+    m.ux = raw[1];
+    m.uy = raw[2];
+    m.uz = raw[3];
+    m.sxx = raw[4];
+    m.syy = raw[5];
+    m.szz = raw[6];
+    m.sxy = raw[7];
+    m.sxz = raw[8];
+    m.syz = raw[9];
+  }
+  return m;
+}
+
+// Physical moments of a cell pair -> raw stored planes (encode3 of hl_common.cuh, per lane).
+template <class S> __device__ __forceinline__ void encode_pair(const Mom3<P2>& m, const Scale& sc, P2 raw[10]) {
+  if constexpr (S::kEncoded) {
+    const P2 iu(sc.inv_u), is(sc.inv_s);
+    raw[0] = m.drho;
+    raw[1] = m.ux * iu;
+    raw[2] = m.uy * iu;
+    raw[3] = m.uz * iu;
+    raw[4] = (m.sxx - m.ux * m.ux) * is;
+    raw[5] = (m.syy - m.uy * m.uy) * is;
+    raw[6] = (m.szz - m.uz * m.uz) * is;
+    raw[7] = (m.sxy - m.ux * m.uy) * is;
+    raw[8] = (m.sxz - m.ux * m.uz) * is;
+    raw[9] = (m.syz - m.uy * m.uz) * is;
+  } else {
+    raw[0] = m.rho;
+    raw[1] = m.ux;
+    raw[2] = m.uy;
+    raw[3] = m.uz;
+    raw[4] = m.sxx;
+    raw[5] = m.syy;
+    raw[6] = m.szz;
+    raw[7] = m.sxy;
+    raw[8] = m.sxz;
+    raw[9] = m.syz;
+  }
+}
+
+// Raw planes of one cell of a staged plane (k-th moment plane at p[k * stride]); a plane
+// outside the domain (or past the last source plane) reads as the zero cell.
+template <class S>
+__device__ __forceinline__ void load_raw(const typename S::T* p0, const typename S::T* p1, int stride, bool in0,
+                                         bool in1, P2 raw[10]) {
+  const float z0 = S::kEncoded ? -1.f : 0.f;  // raw rho plane of the zero cell
+#pragma unroll
+  for (int k = 0; k < 10; ++k) {
+    const float zk = k == 0 ? z0 : 0.f;
+    raw[k] = P2(in0 ? S::to_r(p0[k * stride]) : zk, in1 ? S::to_r(p1[k * stride]) : zk);
+  }
+}
+
 template <class S, int NSTAGE, bool PERIODIC, bool FORCE, bool FLAGS, bool DIAG>
 __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, const __grid_constant__ Maps maps) {
   using T = typename S::T;
-  using R = typename S::R;
+  static_assert(sizeof(typename S::R) == 4, "the paired kernel computes in binary32");
   using G = Geo<T, NSTAGE>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + G::BAR_OFF);
-  R* mb = reinterpret_cast<R*>(smem + G::MB_OFF);
+  P2* mb = reinterpret_cast<P2*>(smem + G::MB_OFF);  // [24 directions][512 destinations]
   __shared__ int box_c[6];  // z lo, z mid, z hi, y lo, y mid, y hi of the current item
 
   const int tid = threadIdx.x;
   const int ty = tid / TZ, tz = tid % TZ;
-  const int dsrc = (ty + 1) * BZ + tz + 1;  // mailbox slot of this thread's interior cell
+  // which y/z neighbours of this thread's cell lie inside the tile
+  const bool yl_ok = ty > 0, yh_ok = ty < TY - 1, zl_ok = tz > 0, zh_ok = tz < TZ - 1;
   // halo cell of threads 0..99: rows y0-1 / y0+16 (34 cells each), columns z0-1 / z0+32
   const bool has_halo = tid < NHALO;
   int hsy = 0, hsz = 0, piece_off = 0, cell_off = 0, mstride = 1, sel_y = -1, sel_z = -1;
@@ -148,11 +257,27 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
     mstride = G::E_ZE;
     sel_z = hi ? 0 : 2;
   }
-  const int h_idx = hsy * BZ + hsz;
+  const int hy = hsy - 1, hz = hsz - 1;  // halo cell in tile coordinates
+  // The halo cell sends one face slice into the tile: a row cell (y0-1 or y0+16) the
+  // populations with c_y = hs, a column cell (z0-1 or z0+32) those with c_z = hs; entry i of
+  // the slice has the other component i - 1. Its mailbox rows and destination slots:
+  const bool h_row = tid < 2 * BZ;
+  const int hs = h_row ? (hy < 0 ? 1 : -1) : (hz < 0 ? 1 : -1);
+  int h_dir[3], h_dst[3];
+  bool h_ok[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int yi = h_row ? hs + 1 : i, zi = h_row ? i : hs + 1;
+    const int idx = yi * 3 + zi;
+    h_dir[i] = idx < 4 ? idx : idx - 1;  // mb_dir(0, yi, zi)
+    const int ddy = hy + yi - 1, ddz = hz + zi - 1;
+    h_ok[i] = has_halo && ddy >= 0 && ddy < TY && ddz >= 0 && ddz < TZ;
+    h_dst[i] = ddy * TZ + ddz;
+  }
   const long long N = a.N;
   const long long plane = (long long)a.ny * a.nz;
   T* post = static_cast<T*>(a.post);
-  const R omega = R(1) / (R(a.vis_shear) * R(3) + R(0.5));
+  const PairConst kc = make_pair_const(1.f / (float(a.vis_shear) * 3.f + 0.5f));
 
   if (tid == 0) {
     for (int k = 0; k < NSTAGE; ++k) mbar_init(saddr(&bars[k]), 1);
@@ -186,6 +311,16 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
     tma_load4(saddr(st + G::OFF_C + 2 * G::B_C), &maps.corner, zl, yh, gx, 0, bar);
     tma_load4(saddr(st + G::OFF_C + 3 * G::B_C), &maps.corner, zh, yh, gx, 0, bar);
   };
+  auto wait_stage = [&](int q_slot, int q_phase) {
+    const unsigned bar = saddr(&bars[q_slot]);
+    long long spin = 0;
+    while (!mbar_try_wait(bar, unsigned(q_phase))) {
+      if (++spin > MAX_SPIN) {  // the copy never landed: report, keep the barriers matched
+        timed_out = true;
+        break;
+      }
+    }
+  };
 
   for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
     const int tile = item % a.n_tiles, chunk = item / a.n_tiles;
@@ -195,6 +330,7 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
     const int hgy = y0 - 1 + hsy, hgz = z0 - 1 + hsz;
     const bool h_in = PERIODIC || (hgy >= 0 && hgy < a.ny && hgz >= 0 && hgz < a.nz);
     const int dy = y0 + ty, dz = z0 + tz;
+    __syncthreads();  // the previous item's readers are done with box_c and the mailbox
     if (tid == 0) {
       int zl = z0 - G::WZ, zh = z0 + TZ, yl = y0 - 1, yh = y0 + TY;
       if (PERIODIC) {
@@ -209,104 +345,158 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
       box_c[3] = yl;
       box_c[4] = y0;
       box_c[5] = yh;
-      // fill the pipeline: planes xb-1 .. xb+NSTAGE-3 into the next NSTAGE-1 slots
+      // fill the pipeline: source planes xb-1 .. into all NSTAGE slots (every slot is free:
+      // the previous item issued nothing beyond its last plane)
       int s = slot;
-      for (int k = 0; k < NSTAGE - 1 && xb - 1 + k <= xe; ++k) {
+      for (int k = 0; k < NSTAGE && xb - 1 + k <= xe; ++k) {
         issue(xb - 1 + k, s);
         s = s + 1 == NSTAGE ? 0 : s + 1;
       }
     }
-    Acc<R> acc_cur, acc_next;
-    acc_cur.zero();
-    acc_next.zero();
-    for (int xs = xb - 1; xs <= xe; ++xs) {
-      __syncthreads();  // the mailbox is free and the stage read last iteration can be refilled
-      if (tid == 0 && xs + NSTAGE - 1 <= xe) issue(xs + NSTAGE - 1, slot == 0 ? NSTAGE - 1 : slot - 1);
-      {
-        const unsigned bar = saddr(&bars[slot]);
-        long long spin = 0;
-        while (!mbar_try_wait(bar, unsigned(phase))) {
-          if (++spin > MAX_SPIN) {  // the copy never landed: report, keep the barriers matched
-            timed_out = true;
-            break;
-          }
-        }
+    // group sums of the previous pair that the next destinations still need: all of c_x = +1,
+    // the second plane's of c_x = 0
+    GroupSums gp_prev;
+    gp_prev.m0 = gp_prev.my = gp_prev.myy = gp_prev.mz = gp_prev.mzz = gp_prev.myz = P2(0.f, 0.f);
+    float z_m0 = 0.f, z_my = 0.f, z_myy = 0.f, z_mz = 0.f, z_mzz = 0.f, z_myz = 0.f;
+
+    // Source planes in pairs (s0, s0 + 1); lane 0 of every P2 is plane s0, lane 1 plane s0 + 1.
+    for (int s0 = xb - 1; s0 <= xe; s0 += 2) {
+      const int s1 = s0 + 1;
+      const bool has1 = s1 <= xe;  // false: lane 1 is past the last source plane
+      const int slot0 = slot, ph0 = phase;
+      slot = slot + 1 == NSTAGE ? 0 : slot + 1;
+      if (slot == 0) phase ^= 1;
+      const int slot1 = slot, ph1 = phase;
+      if (has1) {
+        slot = slot + 1 == NSTAGE ? 0 : slot + 1;
+        if (slot == 0) phase ^= 1;
       }
-      const bool x_in = PERIODIC || (xs >= 0 && xs < a.nx);
-      const unsigned char* stage = smem + slot * G::STAGE_BYTES;
-      {  // interior source cell (tiles are full, so always inside the y/z range)
-        Mom3<R> m;
-        if (x_in) {
-          const T* p = reinterpret_cast<const T*>(stage + G::OFF_MID) + tid;
-          R raw[10];
+      wait_stage(slot0, ph0);
+      if (has1) wait_stage(slot1, ph1);
+      const bool in0 = PERIODIC || (s0 >= 0 && s0 < a.nx);
+      const bool in1 = has1 && (PERIODIC || (s1 >= 0 && s1 < a.nx));
+      const unsigned char* st0 = smem + slot0 * G::STAGE_BYTES;
+      const unsigned char* st1 = smem + slot1 * G::STAGE_BYTES;
+
+      P2 fc[3];  // populations that stay in this column (c_y = c_z = 0)
+      {          // interior source cells (tiles are full, so always inside the y/z range)
+        P2 raw[10];
+        load_raw<S>(reinterpret_cast<const T*>(st0 + G::OFF_MID) + tid, reinterpret_cast<const T*>(st1 + G::OFF_MID) + tid,
+                    G::E_MID, in0, in1, raw);
+        const Coef cf = coefficients(decode_pair<S>(raw, a.sc), kc);
+        P2 f[27];
+        rebuild_pair(cf, kc, f);
 #pragma unroll
-          for (int k = 0; k < 10; ++k) raw[k] = S::to_r(p[k * G::E_MID]);
-          m = decode3<S>(raw, a.sc);
-        } else {
-          m = zero_cell<R>();
+        for (int xi = 0; xi < 3; ++xi) {
+          fc[xi] = f[dir_index(xi - 1, 0, 0)];
+#pragma unroll
+          for (int yi = 0; yi < 3; ++yi)
+#pragma unroll
+            for (int zi = 0; zi < 3; ++zi) {
+              if (yi == 1 && zi == 1) continue;
+              const bool ok = (yi == 0 ? yl_ok : yi == 2 ? yh_ok : true) && (zi == 0 ? zl_ok : zi == 2 ? zh_ok : true);
+              if (ok) mb[mb_dir(xi, yi, zi) * NDST + tid + (yi - 1) * TZ + (zi - 1)] = f[(xi * 3 + yi) * 3 + zi];
+            }
         }
-        R f[27];
-        rebuild_all<R>(m, f);
-#pragma unroll
-        for (int d = 0; d < 27; ++d) mb[d * NSRC + dsrc] = f[d];
       }
       if (has_halo) {
-        Mom3<R> m;
-        if (x_in && h_in) {
-          const T* p = reinterpret_cast<const T*>(stage + piece_off) + cell_off;
-          R raw[10];
+        P2 raw[10];
+        load_raw<S>(reinterpret_cast<const T*>(st0 + piece_off) + cell_off,
+                    reinterpret_cast<const T*>(st1 + piece_off) + cell_off, mstride, in0 && h_in, in1 && h_in, raw);
+        const Coef cf = coefficients(decode_pair<S>(raw, a.sc), kc);
+        P2 f[3][3];
+        rebuild_face(cf, kc, h_row, P2(float(hs), float(hs)), f);
 #pragma unroll
-          for (int k = 0; k < 10; ++k) raw[k] = S::to_r(p[k * mstride]);
-          m = decode3<S>(raw, a.sc);
-        } else {
-          m = zero_cell<R>();
-        }
-        rebuild_slice<R>(m, sel_y, sel_z, [&](int d, R v) { mb[d * NSRC + h_idx] = v; });
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int xi = 0; xi < 3; ++xi)
+            if (h_ok[i]) mb[(xi * 8 + h_dir[i]) * NDST + h_dst[i]] = f[i][xi];
       }
-      __syncthreads();  // mailbox complete
-      Acc<R> acc_new;
-      acc_new.zero();
+      __syncthreads();  // mailbox complete; every thread is done with both stages
+      if (tid == 0) {
+        if (s0 + NSTAGE <= xe) issue(s0 + NSTAGE, slot0);
+        if (has1 && s1 + NSTAGE <= xe) issue(s1 + NSTAGE, slot1);
+      }
+
+      GroupSums g[3];
 #pragma unroll
       for (int xi = 0; xi < 3; ++xi) {
-        R p[3][3];
+        P2 p[3][3];
 #pragma unroll
         for (int yi = 0; yi < 3; ++yi)
 #pragma unroll
           for (int zi = 0; zi < 3; ++zi)
-            p[yi][zi] = mb[((xi * 3 + yi) * 3 + zi) * NSRC + dsrc - (yi - 1) * BZ - (zi - 1)];
-        if (xi == 0) accumulate_group<R>(acc_cur, p, -1);
-        else if (xi == 1) accumulate_group<R>(acc_next, p, 0);
-        else accumulate_group<R>(acc_new, p, 1);
+            p[yi][zi] = (yi == 1 && zi == 1) ? fc[xi] : mb[mb_dir(xi, yi, zi) * NDST + tid];
+        g[xi] = group_sums(p);
       }
-      const int dx = xs - 1;
-      if (dx >= xb) {
-        const long long c = (long long)dx * plane + (long long)dy * a.nz + dz;
-        bool fluid;
-        if (FLAGS) fluid = a.flag[c] == ML_FLUID;
-        else if (PERIODIC) fluid = true;
-        else fluid = dx > 0 && dx < a.nx - 1 && dy > 0 && dy < a.ny - 1 && dz > 0 && dz < a.nz - 1;
-        if (fluid) {
-          R Fx = R(0), Fy = R(0), Fz = R(0);
+      // destinations d0 = s0 - 1 and d1 = s0: c_x = -1 populations from (s0, s1), c_x = +1
+      // from the previous pair (s0 - 2, s0 - 1), c_x = 0 from (s0 - 1, s0)
+      const GroupSums& gm = g[0];
+      Acc<P2> acc;
+      const GroupSums& g0 = g[1];
+      acc.pxx = gm.m0 + gp_prev.m0;
+      acc.rho = acc.pxx + P2(z_m0, g0.m0.x());
+      acc.jx = gp_prev.m0 - gm.m0;
+      acc.jy = (gm.my + gp_prev.my) + P2(z_my, g0.my.x());
+      acc.pxy = gp_prev.my - gm.my;
+      acc.jz = (gm.mz + gp_prev.mz) + P2(z_mz, g0.mz.x());
+      acc.pxz = gp_prev.mz - gm.mz;
+      acc.pyy = (gm.myy + gp_prev.myy) + P2(z_myy, g0.myy.x());
+      acc.pzz = (gm.mzz + gp_prev.mzz) + P2(z_mzz, g0.mzz.x());
+      acc.pyz = (gm.myz + gp_prev.myz) + P2(z_myz, g0.myz.x());
+      gp_prev = g[2];
+      z_m0 = g0.m0.y();
+      z_my = g0.my.y();
+      z_myy = g0.myy.y();
+      z_mz = g0.mz.y();
+      z_mzz = g0.mzz.y();
+      z_myz = g0.myz.y();
+
+      const int d0 = s0 - 1;
+      const bool v0 = d0 >= xb && d0 < xe, v1 = d0 + 1 >= xb && d0 + 1 < xe;
+      if (v0 || v1) {
+        const long long c0 = (long long)d0 * plane + (long long)dy * a.nz + dz, c1 = c0 + plane;
+        bool f0 = v0, f1 = v1;
+        if (FLAGS) {
+          f0 = f0 && a.flag[c0] == ML_FLUID;
+          f1 = f1 && a.flag[c1] == ML_FLUID;
+        } else if (!PERIODIC) {
+          const bool yz = dy > 0 && dy < a.ny - 1 && dz > 0 && dz < a.nz - 1;
+          f0 = f0 && yz && d0 > 0 && d0 < a.nx - 1;
+          f1 = f1 && yz && d0 + 1 > 0 && d0 + 1 < a.nx - 1;
+        }
+        if (f0 || f1) {
+          P2 Fx(0.f, 0.f), Fy(0.f, 0.f), Fz(0.f, 0.f);
           if (FORCE) {
-            Fx = R(a.force[c]);
-            Fy = R(a.force[N + c]);
-            Fz = R(a.force[2 * N + c]);
+            Fx = P2(f0 ? a.force[c0] : 0.f, f1 ? a.force[c1] : 0.f);
+            Fy = P2(f0 ? a.force[N + c0] : 0.f, f1 ? a.force[N + c1] : 0.f);
+            Fz = P2(f0 ? a.force[2 * N + c0] : 0.f, f1 ? a.force[2 * N + c1] : 0.f);
           }
-          const Mom3<R> m = collide<R>(acc_cur, Fx, Fy, Fz, omega);
-          R raw[10];
-          encode3<S>(m, a.sc, raw);
+          const Mom3<P2> m = collide_pair<FORCE>(acc, Fx, Fy, Fz, kc);
+          P2 raw[10];
+          encode_pair<S>(m, a.sc, raw);
+          if (f0) {
 #pragma unroll
-          for (int k = 0; k < 10; ++k) post[k * N + c] = S::from_r(raw[k]);
+            for (int k = 0; k < 10; ++k) post[k * N + c0] = S::from_r(raw[k].x());
+          }
+          if (f1) {
+#pragma unroll
+            for (int k = 0; k < 10; ++k) post[k * N + c1] = S::from_r(raw[k].y());
+          }
           if (DIAG) {
-            mass += double(m.rho);
-            bad += healthy<R>(m) ? 0 : 1;
+            const P2 s = m.ux + m.uy + m.uz + m.sxx + m.syy + m.szz + m.sxy + m.sxz + m.syz;
+            if (f0) {
+              mass += double(m.rho.x());
+              bad += (isfinite(m.rho.x()) && isfinite(s.x()) && m.rho.x() > 0.f) ? 0 : 1;
+            }
+            if (f1) {
+              mass += double(m.rho.y());
+              bad += (isfinite(m.rho.y()) && isfinite(s.y()) && m.rho.y() > 0.f) ? 0 : 1;
+            }
           }
         }
       }
-      acc_cur = acc_next;
-      acc_next = acc_new;
-      slot = slot + 1 == NSTAGE ? 0 : slot + 1;
-      if (slot == 0) phase ^= 1;
+      __syncthreads();  // every thread has read the mailbox: the next pair may overwrite it
     }
   }
   if (timed_out && a.status) atomicExch(a.status, HL_ERR_TIMEOUT);
@@ -442,6 +632,16 @@ int launch(const hl_world3d* w, double vis, const hl_diag* diag, cudaStream_t st
   a.sc = make_scale(w->storage);
   if (DIAG) fill_diag(a, diag);
   auto kern = step_kernel_tma<S, NSTAGE, PERIODIC, FORCE, FLAGS, DIAG>;
+  {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (optin > 0 && G::SMEM > optin) {
+      set_error("d3q27 (tma): %d pipeline stages need %d bytes of shared memory (device limit %d)", NSTAGE, G::SMEM,
+                optin);
+      return HL_ERR_UNSUPPORTED;
+    }
+  }
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
@@ -498,7 +698,7 @@ template <int NS> int launch_ns(const hl_world3d* w, double vis, const hl_diag* 
 }
 
 int launch_step_tma(const hl_world3d* w, double vis, const hl_diag* diag, cudaStream_t st) {
-  // pipeline depth: 4 stages (three planes in flight) unless tuned
+  // pipeline depth: 4 staged planes (the pair being computed and the next pair) unless tuned
   switch (g_tune_d3_stages) {
     case 3: return launch_ns<3>(w, vis, diag, st);
     case 5: return launch_ns<5>(w, vis, diag, st);
