@@ -13,6 +13,12 @@
 namespace hl {
 namespace d3 {
 
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Loop-invariant pairs: lattice weights by number of non-zero velocity components, and the
 // relaxation factors.
 struct PairConst {
@@ -32,10 +38,6 @@ __device__ __forceinline__ PairConst make_pair_const(float omega) {
   k.third = P2(1.0 / 3.0);
   k.half = P2(0.5);
   return k;
-}
-
-__device__ __forceinline__ P2 weight(const PairConst& k, int nnz) {
-  return nnz == 0 ? k.w0 : nnz == 1 ? k.w1 : nnz == 2 ? k.w2 : k.w3;
 }
 
 // Coefficients of the rebuilt deviation g(c) - 1 = A + c.B + sum_a c_a^2 C_aa + sum_{a<b}
@@ -65,7 +67,22 @@ __device__ __forceinline__ Coef coefficients(const Mom3<P2>& m, const PairConst&
   return c;
 }
 
-__device__ __forceinline__ P2 clamp_w(P2 g, P2 w) { return w * fmax(g, P2(-1.f, -1.f)); }
+// w max(g, -1) = max(w g, -w) for w > 0, lane-wise: the clamp takes -w as an immediate.
+template <int NNZ> __device__ __forceinline__ P2 clamp_w(P2 wg) {
+  constexpr float w = NNZ == 0 ? float(8.0 / 27.0) : NNZ == 1 ? float(2.0 / 27.0) : NNZ == 2 ? float(1.0 / 54.0) : float(1.0 / 216.0);
+  return P2(fmaxf(wg.x(), -w), fmaxf(wg.y(), -w));
+}
+
+// The three populations of one (c_y, c_z) with c_x = 0, +1, -1 (deviations f - w) from the
+// c_x = 0 value p and the c_x-linear part q: w_n max(p, -1) and w_{n+1} max(p + Cxx +- q, -1),
+// the latter as w_{n+1} p + w_{n+1} Cxx +- w_{n+1} q (one FFMA2 each).
+template <int N>
+__device__ __forceinline__ void column3(P2 p, P2 q, P2 wn, P2 wn1, P2 wCxx1, P2& f0, P2& fp, P2& fm) {
+  f0 = clamp_w<N>(P2(wn * p));
+  const P2 wpc = wn1 * p + wCxx1;
+  fp = clamp_w<N + 1>(wn1 * q + wpc);
+  fm = clamp_w<N + 1>(wpc - wn1 * q);
+}
 
 // All 27 clamped populations (deviations f - w) of an interior cell pair, f[dir_index].
 __device__ __forceinline__ void rebuild_pair(const Coef& c, const PairConst& k, P2 f[27]) {
@@ -91,16 +108,20 @@ __device__ __forceinline__ void rebuild_pair(const Coef& c, const PairConst& k, 
   Q[0][0] = c.Bx - t1;
   Q[2][0] = c.Bx + t2;
   Q[0][2] = c.Bx - t2;
-#pragma unroll
-  for (int yi = 0; yi < 3; ++yi)
-#pragma unroll
-    for (int zi = 0; zi < 3; ++zi) {
-      const int nyz = (yi != 1) + (zi != 1);
-      const P2 p = P[yi][zi], pc = p + c.Cxx, q = Q[yi][zi];
-      f[(1 * 3 + yi) * 3 + zi] = clamp_w(p, weight(k, nyz));
-      f[(2 * 3 + yi) * 3 + zi] = clamp_w(pc + q, weight(k, nyz + 1));
-      f[(0 * 3 + yi) * 3 + zi] = clamp_w(pc - q, weight(k, nyz + 1));
-    }
+  const P2 wC1 = k.w1 * c.Cxx, wC2 = k.w2 * c.Cxx, wC3 = k.w3 * c.Cxx;
+#define HL_COL3(yi, zi, N, WN, WN1, WC)                                                                \
+  column3<N>(P[yi][zi], Q[yi][zi], WN, WN1, WC, f[(1 * 3 + yi) * 3 + zi], f[(2 * 3 + yi) * 3 + zi], \
+             f[(0 * 3 + yi) * 3 + zi])
+  HL_COL3(1, 1, 0, k.w0, k.w1, wC1);
+  HL_COL3(0, 1, 1, k.w1, k.w2, wC2);
+  HL_COL3(2, 1, 1, k.w1, k.w2, wC2);
+  HL_COL3(1, 0, 1, k.w1, k.w2, wC2);
+  HL_COL3(1, 2, 1, k.w1, k.w2, wC2);
+  HL_COL3(0, 0, 2, k.w2, k.w3, wC3);
+  HL_COL3(0, 2, 2, k.w2, k.w3, wC3);
+  HL_COL3(2, 0, 2, k.w2, k.w3, wC3);
+  HL_COL3(2, 2, 2, k.w2, k.w3, wC3);
+#undef HL_COL3
 }
 
 // The 9 populations a halo cell sends across one face of the tile: the slice with c_u = s
@@ -118,14 +139,10 @@ __device__ __forceinline__ void rebuild_face(const Coef& c, const PairConst& k, 
   const P2 bC = base + Cvv;
   const P2 p[3] = {bC - lin, base, bC + lin};
   const P2 q[3] = {qb - Dxv, qb, qb + Dxv};
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    const int n = 1 + (i != 1);  // non-zero components at c_x = 0
-    const P2 pc = p[i] + c.Cxx;
-    f[i][1] = clamp_w(p[i], weight(k, n));
-    f[i][2] = clamp_w(pc + q[i], weight(k, n + 1));
-    f[i][0] = clamp_w(pc - q[i], weight(k, n + 1));
-  }
+  const P2 wC2 = k.w2 * c.Cxx, wC3 = k.w3 * c.Cxx;
+  column3<2>(p[0], q[0], k.w2, k.w3, wC3, f[0][1], f[0][2], f[0][0]);
+  column3<1>(p[1], q[1], k.w1, k.w2, wC2, f[1][1], f[1][2], f[1][0]);
+  column3<2>(p[2], q[2], k.w2, k.w3, wC3, f[2][1], f[2][2], f[2][0]);
 }
 
 // Regularised collision of a destination pair from its deviation sums (collide in
@@ -136,7 +153,9 @@ __device__ __forceinline__ void rebuild_face(const Coef& c, const PairConst& k, 
 template <bool FORCE>
 __device__ __forceinline__ Mom3<P2> collide_pair(const Acc<P2>& a, P2 Fx, P2 Fy, P2 Fz, const PairConst& k) {
   const P2 rho = a.rho + P2(1.f, 1.f);
-  const P2 inv(__frcp_rn(rho.x()), __frcp_rn(rho.y()));
+  // 1 / rho: hardware estimate, then one Newton step r + r (1 - rho r) on both lanes
+  const P2 r0(rcp_approx(rho.x()), rcp_approx(rho.y()));
+  const P2 inv = r0 * (P2(1.f, 1.f) - rho * r0) + r0;
   P2 ux, uy, uz;
   if (FORCE) {
     ux = (Fx * k.half + a.jx) * inv;

@@ -201,16 +201,20 @@ template <class S> __device__ __forceinline__ void encode_pair(const Mom3<P2>& m
   }
 }
 
-// Raw planes of one cell of a staged plane (k-th moment plane at p[k * stride]); a plane
-// outside the domain (or past the last source plane) reads as the zero cell.
-template <class S>
+// Raw planes of one cell of a staged plane (k-th moment plane at p[k * stride]). A cell
+// outside a walled domain must read as the zero cell. The TMA unit zero-fills boxes outside
+// the tensor, which IS the zero cell of float32 storage (rho = 0, drho = -1); the encoded
+// storages store rho - 1 and need the select (SEL). A lane past the last source plane of an
+// item holds stale data: its populations only reach destinations that are never stored.
+template <class S, bool SEL>
 __device__ __forceinline__ void load_raw(const typename S::T* p0, const typename S::T* p1, int stride, bool in0,
                                          bool in1, P2 raw[10]) {
   const float z0 = S::kEncoded ? -1.f : 0.f;  // raw rho plane of the zero cell
 #pragma unroll
   for (int k = 0; k < 10; ++k) {
     const float zk = k == 0 ? z0 : 0.f;
-    raw[k] = P2(in0 ? S::to_r(p0[k * stride]) : zk, in1 ? S::to_r(p1[k * stride]) : zk);
+    const float v0 = S::to_r(p0[k * stride]), v1 = S::to_r(p1[k * stride]);
+    raw[k] = SEL ? P2(in0 ? v0 : zk, in1 ? v1 : zk) : P2(v0, v1);
   }
 }
 
@@ -219,11 +223,11 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
   using T = typename S::T;
   static_assert(sizeof(typename S::R) == 4, "the paired kernel computes in binary32");
   using G = Geo<T, NSTAGE>;
+  constexpr bool SEL = S::kEncoded && !PERIODIC;  // see load_raw
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + G::BAR_OFF);
   P2* mb = reinterpret_cast<P2*>(smem + G::MB_OFF);  // [24 directions][512 destinations]
-  __shared__ int box_c[6];  // z lo, z mid, z hi, y lo, y mid, y hi of the current item
 
   const int tid = threadIdx.x;
   const int ty = tid / TZ, tz = tid % TZ;
@@ -288,17 +292,33 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
   double mass = 0.0;
   int bad = 0;
   bool timed_out = false;
-  // running plane counter: plane q is staged in slot q % NSTAGE and its mbarrier completes
-  // for the (q / NSTAGE)-th time
-  int slot = 0, phase = 0;
-
-  auto issue = [&](int xs, int q_slot) {
-    // thread 0: nine boxes of plane xs into stage q_slot
+  // The CTA's source planes form one sequence over all its items (per item xb-1 .. xe).
+  // Plane q of the sequence is staged in slot q % NSTAGE, whose mbarrier completes for the
+  // (q / NSTAGE)-th time. Thread 0 produces the sequence NSTAGE planes ahead of the
+  // consumers, across item boundaries, so a new item starts with its planes already staged.
+  int slot = 0, phase = 0;                                  // consumer position
+  int p_item = blockIdx.x, p_x = 0, p_xe = 0, p_slot = 0;  // producer position (thread 0)
+  int p_y0 = 0, p_z0 = 0;
+  auto item_range = [&](int item, int& y0, int& z0, int& xb, int& xe) {
+    const int tile = item % a.n_tiles, chunk = item / a.n_tiles;
+    y0 = (tile / a.tiles_z) * TY;
+    z0 = (tile % a.tiles_z) * TZ;
+    xb = chunk * a.chunk_len;
+    xe = min(xb + a.chunk_len, a.nx);
+  };
+  auto issue = [&](int xs, int q_slot, int y0, int z0) {
+    // nine boxes of plane xs of the tile at (y0, z0) into stage q_slot
     unsigned char* st = smem + q_slot * G::STAGE_BYTES;
     const unsigned bar = saddr(&bars[q_slot]);
     int gx = xs;
     if (PERIODIC) gx = gx < 0 ? gx + a.nx : (gx >= a.nx ? gx - a.nx : gx);
-    const int zl = box_c[0], z0 = box_c[1], zh = box_c[2], yl = box_c[3], y0 = box_c[4], yh = box_c[5];
+    int zl = z0 - G::WZ, zh = z0 + TZ, yl = y0 - 1, yh = y0 + TY;
+    if (PERIODIC) {
+      if (zl < 0) zl += a.nz;
+      if (zh >= a.nz) zh -= a.nz;
+      if (yl < 0) yl += a.ny;
+      if (yh >= a.ny) yh -= a.ny;
+    }
     fence_proxy_async();
     mbar_expect_tx(bar, G::TX_BYTES);
     tma_load4(saddr(st + G::OFF_MID), &maps.mid, z0, y0, gx, 0, bar);
@@ -311,6 +331,26 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
     tma_load4(saddr(st + G::OFF_C + 2 * G::B_C), &maps.corner, zl, yh, gx, 0, bar);
     tma_load4(saddr(st + G::OFF_C + 3 * G::B_C), &maps.corner, zh, yh, gx, 0, bar);
   };
+  auto produce = [&](int n) {  // thread 0: the next n planes of the sequence
+    for (int k = 0; k < n && p_item < a.n_items; ++k) {
+      issue(p_x, p_slot, p_y0, p_z0);
+      p_slot = p_slot + 1 == NSTAGE ? 0 : p_slot + 1;
+      if (++p_x > p_xe) {
+        p_item += gridDim.x;
+        if (p_item < a.n_items) {
+          int xb;
+          item_range(p_item, p_y0, p_z0, xb, p_xe);
+          p_x = xb - 1;
+        }
+      }
+    }
+  };
+  if (tid == 0 && p_item < a.n_items) {
+    int xb;
+    item_range(p_item, p_y0, p_z0, xb, p_xe);
+    p_x = xb - 1;
+    produce(NSTAGE);
+  }
   auto wait_stage = [&](int q_slot, int q_phase) {
     const unsigned bar = saddr(&bars[q_slot]);
     long long spin = 0;
@@ -323,36 +363,11 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
   };
 
   for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
-    const int tile = item % a.n_tiles, chunk = item / a.n_tiles;
-    const int y0 = (tile / a.tiles_z) * TY, z0 = (tile % a.tiles_z) * TZ;
-    const int xb = chunk * a.chunk_len;
-    const int xe = min(xb + a.chunk_len, a.nx);
+    int y0, z0, xb, xe;
+    item_range(item, y0, z0, xb, xe);
     const int hgy = y0 - 1 + hsy, hgz = z0 - 1 + hsz;
     const bool h_in = PERIODIC || (hgy >= 0 && hgy < a.ny && hgz >= 0 && hgz < a.nz);
     const int dy = y0 + ty, dz = z0 + tz;
-    __syncthreads();  // the previous item's readers are done with box_c and the mailbox
-    if (tid == 0) {
-      int zl = z0 - G::WZ, zh = z0 + TZ, yl = y0 - 1, yh = y0 + TY;
-      if (PERIODIC) {
-        if (zl < 0) zl += a.nz;
-        if (zh >= a.nz) zh -= a.nz;
-        if (yl < 0) yl += a.ny;
-        if (yh >= a.ny) yh -= a.ny;
-      }
-      box_c[0] = zl;
-      box_c[1] = z0;
-      box_c[2] = zh;
-      box_c[3] = yl;
-      box_c[4] = y0;
-      box_c[5] = yh;
-      // fill the pipeline: source planes xb-1 .. into all NSTAGE slots (every slot is free:
-      // the previous item issued nothing beyond its last plane)
-      int s = slot;
-      for (int k = 0; k < NSTAGE && xb - 1 + k <= xe; ++k) {
-        issue(xb - 1 + k, s);
-        s = s + 1 == NSTAGE ? 0 : s + 1;
-      }
-    }
     // group sums of the previous pair that the next destinations still need: all of c_x = +1,
     // the second plane's of c_x = 0
     GroupSums gp_prev;
@@ -381,7 +396,7 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
       P2 fc[3];  // populations that stay in this column (c_y = c_z = 0)
       {          // interior source cells (tiles are full, so always inside the y/z range)
         P2 raw[10];
-        load_raw<S>(reinterpret_cast<const T*>(st0 + G::OFF_MID) + tid, reinterpret_cast<const T*>(st1 + G::OFF_MID) + tid,
+        load_raw<S, SEL>(reinterpret_cast<const T*>(st0 + G::OFF_MID) + tid, reinterpret_cast<const T*>(st1 + G::OFF_MID) + tid,
                     G::E_MID, in0, in1, raw);
         const Coef cf = coefficients(decode_pair<S>(raw, a.sc), kc);
         P2 f[27];
@@ -401,7 +416,7 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
       }
       if (has_halo) {
         P2 raw[10];
-        load_raw<S>(reinterpret_cast<const T*>(st0 + piece_off) + cell_off,
+        load_raw<S, SEL>(reinterpret_cast<const T*>(st0 + piece_off) + cell_off,
                     reinterpret_cast<const T*>(st1 + piece_off) + cell_off, mstride, in0 && h_in, in1 && h_in, raw);
         const Coef cf = coefficients(decode_pair<S>(raw, a.sc), kc);
         P2 f[3][3];
@@ -413,10 +428,7 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
             if (h_ok[i]) mb[(xi * 8 + h_dir[i]) * NDST + h_dst[i]] = f[i][xi];
       }
       __syncthreads();  // mailbox complete; every thread is done with both stages
-      if (tid == 0) {
-        if (s0 + NSTAGE <= xe) issue(s0 + NSTAGE, slot0);
-        if (has1 && s1 + NSTAGE <= xe) issue(s1 + NSTAGE, slot1);
-      }
+      if (tid == 0) produce(has1 ? 2 : 1);
 
       GroupSums g[3];
 #pragma unroll
