@@ -46,18 +46,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+# DRAM bytes (read + write) per cell of one stream-collide launch, from one ncu capture of
+# the 256^3 bench workload (profiles/d3q27_stream_collide_tma_256_dram.md).
+DRAM_BYTES_PER_CELL = {"float32": 1320.4e6 / 256 ** 3, "float16": 644.9e6 / 256 ** 3}
+
+
 def profile_traffic(n, storage):
-    """dram bytes per launch of the stream-collide kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "d3q27_stream_collide_traffic.json")
-    if not os.path.exists(p):
-        return None
-    with open(p) as f:
-        d = json.load(f)
-    rec = d.get(storage)
-    if not rec:
-        return None
-    # traffic scales with the cells a launch processes
-    return float(rec["dram_bytes_per_cell"]) * n ** 3
+    """dram bytes per launch of the stream-collide kernel (scaled by the cells per launch)."""
+    per_cell = DRAM_BYTES_PER_CELL.get(storage)
+    return None if per_cell is None else per_cell * n ** 3
 
 
 class ClockSampler:
