@@ -10,8 +10,9 @@
  *  - All pointers are device pointers unless the name ends in _host. The caller owns every
  *    buffer (fields live in PyTorch tensors); the library allocates nothing in step calls.
  *  - Every call takes the CUDA stream to run on and performs no host synchronisation and no
- *    allocation. hl_d3q27_stream_collide, hl_d3q27_apply_bc, the hl_d2q9_step* calls and the
- *    init calls can be captured into a CUDA graph.
+ *    allocation. hl_d3q27_stream_collide, hl_d3q27_solid_links, hl_d3q27_apply_bc, the
+ *    hl_d2q9_step* calls, the hl_couple* calls and the init calls can be captured into a
+ *    CUDA graph.
  *  - Return value: HL_OK (0) or a negative hl_status. hl_last_error() gives a message.
  *    Nothing throws across the ABI.
  *
@@ -159,6 +160,90 @@ HL_API int hl_d3q27_init_tgv(int nx, int ny, int nz, hl_storage storage, void* m
 
 /* Replaces InitBoundary3D (envs/lbm3d/lbm_func_3d.py:13-19). */
 HL_API int hl_d3q27_init_boundary(int nx, int ny, int nz, int32_t* flag, hl_stream stream);
+
+/* Immersed triangle-mesh solids of one 3D world (HomeFlow3D's per-solid fields,
+ * envs/lbm3d/lbm_core_3d.py:91-119). Solid k's mesh is the triangles
+ * tris[tri_offset[k] .. tri_offset[k+1]) in its body frame, vertices already scaled by
+ * lbm_scale * nx (create_solid_from_mesh, lbm_solver_3d.py:166-196); a solid with no
+ * triangles is an unset mesh id and is skipped. Transforms are p (3) then q (x, y, z, w). */
+typedef struct {
+  int n_objects;             /* <= 64 */
+  float max_bound_radius;    /* host copy of max(bound_radius): sizes the band launch */
+  const int32_t* tri_offset; /* [n+1] */
+  const float* tris;         /* [total][3][3] */
+  const float* transforms;   /* [n][7] mesh_transforms */
+  const float* transforms_last; /* [n][7] mesh_transforms_last */
+  const int32_t* initialized;   /* [n] mesh_transforms_initialized */
+  const float* scale_sizes;  /* [n][3] mesh_scale_sizes */
+  const float* position;     /* [n][3] solid_position */
+  const float* bound_radius; /* [n] solid_bound_radius */
+  const float* linear_v;     /* [n][3] */
+  const float* angle_v;      /* [n][3] */
+  double* loads64;           /* [n][6] scratch: force then torque summed in binary64 */
+  float* force;              /* [n][3] solid_force (out) */
+  float* torque;             /* [n][3] solid_torque (out) */
+} hl_solids3d;
+
+/* The solid part of one stream_and_collide_3d step (envs/lbm3d/lbm_func_3d.py:364-604) and
+ * init_force_3d_batch (736-747). Call it after hl_d3q27_stream_collide and before
+ * hl_d3q27_apply_bc of the same step, on the same world. It zeroes the loads, then recomputes
+ * post for every fluid cell within bound_radius + 2 of a solid (the narrow band, 387-393):
+ * links whose backward ray hits a mesh within one lattice step (get_cutcell_multi_3d,
+ * 254-316; Moller-Trumbore, double-sided, closest hit) take the wall population rebuilt with
+ * the wall velocity (452-489, not clamped), the others the clamped neighbour population
+ * (525-526); the momentum exchange and its torque about solid_position (490-511) are summed
+ * per solid in binary64 and copied to force / torque in binary32. */
+HL_API int hl_d3q27_solid_links(const hl_world3d* w, double vis_shear, const hl_solids3d* s, hl_stream stream);
+
+/* ------------------------------------------------------------------ coupling
+ * The MuJoCo-Warp coupling kernels of the environments, over batched per-world arrays:
+ * a per-solid array of nworld worlds is [nworld][n_objects][...] with world stride
+ * n_objects * components. MuJoCo buffers are borrowed as they are: xipos [nworld][nbody][3],
+ * xquat [nworld][nbody][4] (w, x, y, z), xfrc [nworld][nbody][6] (force then torque). */
+
+/* extract_body_states(_3d) (envs/lbm/lbm_fluid_env_func.py:8-24,
+ * envs/lbm3d/lbm_fluid_env_3d_func.py:11-36): pos_out [nworld][nsel][3] and quat_out
+ * [nworld][nsel][4] from the bodies body_ids[nsel]. */
+HL_API int hl_couple_body_states(int nworld, int nbody, int nsel, const float* xipos, const float* xquat,
+                                 const int32_t* body_ids, float* pos_out, float* quat_out, hl_stream stream);
+
+/* convert_and_update_solid_batch_3d (lbm_fluid_env_3d_func.py:42-100): for each world and
+ * selected solid, solid_position = (pos - mujoco_origin) * scale + lbm_origin, the
+ * quaternion copied, mesh_transforms_last <- mesh_transforms (once initialised) and the new
+ * transform (p, q(x, y, z, w)); the first call sets last = current and initialized = 1.
+ * position [nworld][n][3], quaternion [nworld][n][4], transforms / transforms_last
+ * [nworld][n][7], initialized [nworld][n]; origins [nsel][3], scales [nsel]. */
+HL_API int hl_couple3d_update_solids(int nworld, int n_objects, int nsel, const int32_t* solid_ids,
+                                     const float* mj_pos, const float* mj_quat, const float* mujoco_origins,
+                                     const float* lbm_origins, const float* scales, float* position,
+                                     float* quaternion, float* transforms, float* transforms_last,
+                                     int32_t* initialized, hl_stream stream);
+
+/* convert_and_update_solid_batch_2d (lbm_fluid_env_func.py:72-105): solid_position
+ * [nworld][n][2] = (pos.xy - origin) * scale + lbm_origin, solid_angle [nworld][n] = the yaw
+ * atan2(2 (w z + x y), 1 - 2 (y^2 + z^2)); origins [nsel][2]. */
+HL_API int hl_couple2d_update_solids(int nworld, int n_objects, int nsel, const int32_t* solid_ids,
+                                     const float* mj_pos, const float* mj_quat, const float* mujoco_origins,
+                                     const float* lbm_origins, const float* scales, float* position, float* angle,
+                                     hl_stream stream);
+
+/* Loads of the selected solids for MuJoCo, [nworld][nsel][3] each:
+ *   mode 0, extract_forces_torques_physical_3d (lbm_fluid_env_3d_func.py:138-178):
+ *          force * force_conv, torque * torque_conv (force / torque [nworld][n][3]);
+ *   mode 1, extract_forces_torques_batch_3d (104-135): force / scale, torque / scale^2;
+ *   mode 2, extract_forces_torques_batch (lbm_fluid_env_func.py:51-69), 2D: force is
+ *          (solid_forcex, solid_forcey, 0) / scale and torque (0, 0, torque / scale), read from
+ *          force = per world the three planes [nworld][3][n] solid_forcex, solid_forcey,
+ *          torque (the torque argument is unused and may be NULL).
+ * scales [nsel] (modes 1, 2). */
+HL_API int hl_couple_loads(int mode, int nworld, int n_objects, int nsel, const int32_t* solid_ids,
+                           const float* force, const float* torque, const float* scales, float force_conv,
+                           float torque_conv, float* forces_out, float* torques_out, hl_stream stream);
+
+/* fill_xfrc_kernel / fill_xfrc_3d_kernel (lbm_fluid_env_func.py:27-48,
+ * lbm_fluid_env_3d_func.py:181-210): xfrc[w][body_ids[i]] = (forces[w][i], torques[w][i]). */
+HL_API int hl_couple_fill_xfrc(int nworld, int nbody, int nsel, const int32_t* body_ids, const float* forces,
+                               const float* torques, float* xfrc, hl_stream stream);
 
 /* ------------------------------------------------------------------ D2Q9 */
 /* One D2Q9 world (HomeFlow, envs/lbm/lbm_core.py:17-88); cur/post as for D3Q27. */

@@ -41,6 +41,14 @@ class hl_diag(Structure):
                 ("health", c_void_p)]
 
 
+class hl_solids3d(Structure):
+    _fields_ = [("n_objects", c_int), ("max_bound_radius", c_float), ("tri_offset", c_void_p), ("tris", c_void_p),
+                ("transforms", c_void_p), ("transforms_last", c_void_p), ("initialized", c_void_p),
+                ("scale_sizes", c_void_p), ("position", c_void_p), ("bound_radius", c_void_p),
+                ("linear_v", c_void_p), ("angle_v", c_void_p), ("loads64", c_void_p), ("force", c_void_p),
+                ("torque", c_void_p)]
+
+
 class hl_world2d(Structure):
     _fields_ = [("nx", c_int), ("ny", c_int), ("storage", hl_storage), ("cur", c_void_p),
                 ("post", c_void_p), ("flag", c_void_p), ("forcex", c_void_p), ("forcey", c_void_p),
@@ -75,6 +83,13 @@ _SIGS = {
     "hl_d3q27_scratch_bytes": ([POINTER(hl_world3d)], c_size_t),
     "hl_d3q27_stream_collide_noalloc": ([POINTER(hl_world3d), c_double, c_void_p, c_void_p, c_void_p], c_int),
     "hl_d3q27_bc_scratch_bytes": ([POINTER(hl_world3d)], c_size_t),
+    "hl_d3q27_solid_links": ([POINTER(hl_world3d), c_double, POINTER(hl_solids3d), c_void_p], c_int),
+    "hl_couple_body_states": ([c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int),
+    "hl_couple3d_update_solids": ([c_int, c_int, c_int] + [c_void_p] * 12, c_int),
+    "hl_couple2d_update_solids": ([c_int, c_int, c_int] + [c_void_p] * 9, c_int),
+    "hl_couple_loads": ([c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_float,
+                         c_void_p, c_void_p, c_void_p], c_int),
+    "hl_couple_fill_xfrc": ([c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int),
     "hl_d3q27_init_uniform": ([c_int, c_int, c_int, hl_storage, c_void_p, c_void_p, c_void_p, c_float,
                                c_float, c_float, c_void_p], c_int),
     "hl_d3q27_init_tgv": ([c_int, c_int, c_int, hl_storage, c_void_p, c_void_p, c_float, c_void_p], c_int),

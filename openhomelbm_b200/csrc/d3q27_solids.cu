@@ -1,0 +1,383 @@
+// Immersed triangle-mesh solids of the D3Q27 step (sm_100a): the near-solid part of
+// stream_and_collide_3d (envs/lbm3d/lbm_func_3d.py:364-604).
+//
+// The stream-collide kernels (d3q27.cu, d3q27_tma.cu) update every fluid cell as if no solid
+// existed. This file then recomputes the narrow band, the fluid cells within
+// bound_radius + 2 of a solid (387-393), with the reference's per-link logic:
+//   * the link's backward ray cell -> cell - c_i is cast against every solid near the cell
+//     (get_cutcell_multi_3d, 254-316) in the solid's body frame, scaled by mesh_scale_sizes;
+//     the closest hit with 0 <= t <= 1 wins;
+//   * a cut link takes the population rebuilt from the cell's own density and stress with the
+//     wall velocity of the hit point (452-489, not clamped); the momentum exchange against
+//     the cell's own opposite population and its torque about solid_position (490-511) go to
+//     the solid's loads;
+//   * every other link takes the neighbour's clamped population (525-526);
+// followed by the regularised collision (564-604). The band overwrites the cells' post values
+// written by the plain kernel; both read only the current buffer.
+//
+// Launch: one block row per solid (blockIdx.y), covering that solid's bounding box of the
+// band; a cell near several solids is handled by the lowest-numbered one. Loads are summed
+// per block in shared memory and per solid in binary64 global memory.
+//
+// Ray-triangle test: Moller & Trumbore, "Fast, minimum storage ray-triangle intersection"
+// (1997), double-sided, closest hit with 0 <= t <= max_t = 2 (the reference's mesh query
+// bound, lbm_func_3d.py:308). Brute force over the solid's triangles: the band is small and
+// every thread of a warp reads the same triangle, so the loads broadcast.
+
+#include <cmath>
+
+#include "hl_common.cuh"
+
+namespace hl {
+namespace d3s {
+
+constexpr int MAX_SOLIDS = 64;
+constexpr int BLOCK = 128;
+
+// D3Q27 velocities in the reference's order (envs/lbm3d/lbm_core_3d.py:12-35).
+__constant__ signed char c_cx[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
+__constant__ signed char c_cy[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1};
+__constant__ signed char c_cz[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
+
+template <class R> __device__ __forceinline__ R weight(int i) {
+  const int n = (c_cx[i] != 0) + (c_cy[i] != 0) + (c_cz[i] != 0);
+  return n == 0 ? R(8.0 / 27.0) : n == 1 ? R(2.0 / 27.0) : n == 2 ? R(1.0 / 54.0) : R(1.0 / 216.0);
+}
+__device__ __forceinline__ int inverse(int i) { return i == 0 ? 0 : (i & 1) ? i + 1 : i - 1; }
+
+template <class R> struct V3 {
+  R x, y, z;
+};
+template <class R> struct Xf {
+  V3<R> p;
+  R qx, qy, qz, qw;
+};
+
+// Rotation by a unit quaternion: v (2 w^2 - 1) + 2 w (q_v x v) + 2 (q_v . v) q_v.
+template <class R> __device__ __forceinline__ V3<R> qrot(R qx, R qy, R qz, R qw, V3<R> v) {
+  const R c = R(2) * qw * qw - R(1);
+  const R d = R(2) * (qx * v.x + qy * v.y + qz * v.z);
+  const R e = R(2) * qw;
+  const R cx = qy * v.z - qz * v.y, cy = qz * v.x - qx * v.z, cz = qx * v.y - qy * v.x;
+  return {v.x * c + cx * e + qx * d, v.y * c + cy * e + qy * d, v.z * c + cz * e + qz * d};
+}
+template <class R> __device__ __forceinline__ Xf<R> load_xf(const float* t) {
+  return {{R(t[0]), R(t[1]), R(t[2])}, R(t[3]), R(t[4]), R(t[5]), R(t[6])};
+}
+template <class R> __device__ __forceinline__ Xf<R> xinv(const Xf<R>& t) {
+  const V3<R> p = qrot(-t.qx, -t.qy, -t.qz, t.qw, t.p);
+  return {{-p.x, -p.y, -p.z}, -t.qx, -t.qy, -t.qz, t.qw};
+}
+template <class R> __device__ __forceinline__ V3<R> xpoint(const Xf<R>& t, V3<R> v) {
+  const V3<R> r = qrot(t.qx, t.qy, t.qz, t.qw, v);
+  return {r.x + t.p.x, r.y + t.p.y, r.z + t.p.z};
+}
+
+// Closest double-sided hit 0 <= t <= max_t of the ray o + t d with the triangles.
+template <class R>
+__device__ bool ray_mesh(const float* tri, int ntri, V3<R> o, V3<R> d, R max_t, R* t_out) {
+  bool hit = false;
+  R best = R(0);
+  for (int k = 0; k < ntri; ++k) {
+    const float* v = tri + 9 * k;
+    const R v0x = R(v[0]), v0y = R(v[1]), v0z = R(v[2]);
+    const R e1x = R(v[3]) - v0x, e1y = R(v[4]) - v0y, e1z = R(v[5]) - v0z;
+    const R e2x = R(v[6]) - v0x, e2y = R(v[7]) - v0y, e2z = R(v[8]) - v0z;
+    const R px = d.y * e2z - d.z * e2y, py = d.z * e2x - d.x * e2z, pz = d.x * e2y - d.y * e2x;
+    const R det = e1x * px + e1y * py + e1z * pz;
+    if (det == R(0)) continue;
+    const R inv = R(1) / det;
+    const R sx = o.x - v0x, sy = o.y - v0y, sz = o.z - v0z;
+    const R u = (sx * px + sy * py + sz * pz) * inv;
+    if (u < R(0) || u > R(1)) continue;
+    const R qx = sy * e1z - sz * e1y, qy = sz * e1x - sx * e1z, qz = sx * e1y - sy * e1x;
+    const R w = (d.x * qx + d.y * qy + d.z * qz) * inv;
+    if (w < R(0) || u + w > R(1)) continue;
+    const R t = (e2x * qx + e2y * qy + e2z * qz) * inv;
+    if (t < R(0) || t > max_t) continue;
+    if (!hit || t < best) {
+      best = t;
+      hit = true;
+    }
+  }
+  *t_out = best;
+  return hit;
+}
+
+template <class R> __device__ __forceinline__ R vlen(R x, R y, R z) { return sqrt(x * x + y * y + z * z); }
+
+// mlCalEquilibrium3D_s (lbm_func_3d.py:224-251) for direction (dx, dy, dz) with weight wi.
+template <class R>
+__device__ __forceinline__ R feq(R rho, R ux, R uy, R uz, R Sxx, R Sxy, R Sxz, R Syy, R Syz, R Szz, R dx, R dy, R dz,
+                                 R wi) {
+  const R cu = dx * ux + dy * uy + dz * uz;
+  const R usq = ux * ux + uy * uy + uz * uz;
+  const R third = R(1.0 / 3.0);
+  const R Qxx = dx * dx - third, Qyy = dy * dy - third, Qzz = dz * dz - third;
+  const R f_neq = R(1.5) * (Qxx * Sxx + Qyy * Syy + Qzz * Szz + R(2) * (dx * dy * Sxy + dx * dz * Sxz + dy * dz * Syz));
+  return wi * rho * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq + f_neq);
+}
+
+struct Args {
+  hl_world3d w;
+  double vis_shear;
+  hl_solids3d s;
+  Scale sc;
+  int box_side;  // cells per side of the largest band box the launch covers
+};
+
+template <class S> __device__ __forceinline__ Mom3<typename S::R> load_cell(const Args& a, long long N, long long c) {
+  using R = typename S::R;
+  using T = typename S::T;
+  const T* cur = static_cast<const T*>(a.w.cur);
+  R raw[10];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) raw[k] = S::to_r(cur[k * N + c]);
+  return decode3<S>(raw, a.sc);
+}
+
+// Index of the first solid (with a mesh) within bound_radius + 2 of the cell, or -1.
+template <class R> __device__ __forceinline__ int first_near(const hl_solids3d& s, R x, R y, R z) {
+  for (int k = 0; k < s.n_objects; ++k) {
+    if (s.tri_offset[k + 1] == s.tri_offset[k]) continue;
+    const R d = vlen(x - R(s.position[3 * k]), y - R(s.position[3 * k + 1]), z - R(s.position[3 * k + 2]));
+    if (d <= R(s.bound_radius[k]) + R(2)) return k;
+  }
+  return -1;
+}
+
+template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __grid_constant__ Args a) {
+  using R = typename S::R;
+  using T = typename S::T;
+  __shared__ double acc[MAX_SOLIDS * 6];
+  const hl_solids3d& s = a.s;
+  const int n = s.n_objects;
+  for (int k = threadIdx.x; k < 6 * n; k += blockDim.x) acc[k] = 0.0;
+  __syncthreads();
+
+  const int k0 = blockIdx.y;
+  const int nx = a.w.nx, ny = a.w.ny, nz = a.w.nz;
+  const long long N = (long long)nx * ny * nz;
+  bool any = false;
+  // bounding box of solid k0's band, clipped to the grid
+  const float px = s.position[3 * k0], py = s.position[3 * k0 + 1], pz = s.position[3 * k0 + 2];
+  const float r = s.bound_radius[k0] + 2.f;
+  const int side = a.box_side;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s.tri_offset[k0 + 1] > s.tri_offset[k0] && isfinite(px) && isfinite(py) && isfinite(pz) && isfinite(r) &&
+      idx < (long long)side * side * side) {
+    const int bx = int(floorf(px - r)), by = int(floorf(py - r)), bz = int(floorf(pz - r));
+    const int x = bx + int(idx / ((long long)side * side)), y = by + int((idx / side) % side), z = bz + int(idx % side);
+    const bool inside = x >= 0 && x < nx && y >= 0 && y < ny && z >= 0 && z < nz;
+    const long long c = ((long long)x * ny + y) * nz + z;
+    const bool fluid = inside && (a.w.flag == nullptr || a.w.flag[c] == ML_FLUID) &&
+                       (a.w.flag != nullptr || a.w.periodic || (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1));
+    if (fluid && first_near<R>(s, R(x), R(y), R(z)) == k0) {
+      any = true;
+      const Mom3<R> mc = load_cell<S>(a, N, c);
+      R rho_acc = 0, uxp = 0, uxm = 0, uyp = 0, uym = 0, uzp = 0, uzm = 0, pixx = 0, piyy = 0, pizz = 0;
+      R pixy_p = 0, pixy_m = 0, pixz_p = 0, pixz_m = 0, piyz_p = 0, piyz_m = 0;
+      for (int i = 0; i < 27; ++i) {
+        const int ix = c_cx[i], iy = c_cy[i], iz = c_cz[i];
+        const R dx = R(ix), dy = R(iy), dz = R(iz);
+        const R wi = weight<R>(i);
+        int xn = x - ix, yn = y - iy, zn = z - iz;
+        if (a.w.periodic) {
+          xn = wrap(xn, nx);
+          yn = wrap(yn, ny);
+          zn = wrap(zn, nz);
+        }
+        R pop = R(0);
+        if (xn >= 0 && xn < nx && yn >= 0 && yn < ny && zn >= 0 && zn < nz) {
+          // get_cutcell_multi_3d: the closest hit in [0, 1] over the solids near the cell
+          R cut = R(-1);
+          int sid = -1;
+          const V3<R> cell{R(x), R(y), R(z)};
+          const V3<R> dir{-dx, -dy, -dz};
+          for (int k = 0; k < n; ++k) {
+            const int t0 = s.tri_offset[k], ntri = s.tri_offset[k + 1] - t0;
+            if (ntri == 0) continue;
+            if (vlen(cell.x - R(s.position[3 * k]), cell.y - R(s.position[3 * k + 1]), cell.z - R(s.position[3 * k + 2])) >
+                R(s.bound_radius[k]) + R(2))
+              continue;
+            const Xf<R> inv = xinv(load_xf<R>(s.transforms + 7 * k));
+            const V3<R> lo = xpoint(inv, cell);
+            const V3<R> ld = qrot(inv.qx, inv.qy, inv.qz, inv.qw, dir);
+            const R sx = R(s.scale_sizes[3 * k]), sy = R(s.scale_sizes[3 * k + 1]), sz = R(s.scale_sizes[3 * k + 2]);
+            R t;
+            if (ray_mesh<R>(s.tris + 9ll * t0, ntri, {lo.x / sx, lo.y / sy, lo.z / sz}, {ld.x / sx, ld.y / sy, ld.z / sz},
+                            R(2), &t)) {
+              if ((cut < R(0) || t < cut) && t >= R(0) && t <= R(1)) {
+                cut = t;
+                sid = k;
+              }
+            }
+          }
+          if (sid >= 0) {
+            const Xf<R> tc = load_xf<R>(s.transforms + 7 * sid);
+            const Xf<R> tl = load_xf<R>(s.transforms_last + 7 * sid);
+            const V3<R> hit{cell.x + dir.x * cut, cell.y + dir.y * cut, cell.z + dir.z * cut};
+            const V3<R> hl = xpoint(xinv(tc), hit);
+            V3<R> up;
+            const R spx = R(s.position[3 * sid]), spy = R(s.position[3 * sid + 1]), spz = R(s.position[3 * sid + 2]);
+            if (s.initialized[sid] > 0) {
+              const V3<R> pc = xpoint(tc, hl), pl = xpoint(tl, hl);
+              up = {pc.x - pl.x, pc.y - pl.y, pc.z - pl.z};
+            } else {
+              const R ax = R(s.angle_v[3 * sid]), ay = R(s.angle_v[3 * sid + 1]), az = R(s.angle_v[3 * sid + 2]);
+              const R rx = hit.x - spx, ry = hit.y - spy, rz = hit.z - spz;
+              up = {R(s.linear_v[3 * sid]) + (ay * rz - az * ry), R(s.linear_v[3 * sid + 1]) + (az * rx - ax * rz),
+                    R(s.linear_v[3 * sid + 2]) + (ax * ry - ay * rx)};
+            }
+            const R rx = hit.x - spx, ry = hit.y - spy, rz = hit.z - spz;
+            const R Sxx_s = up.x * up.x + mc.sxx - mc.ux * mc.ux;
+            const R Sxy_s = up.x * up.y + mc.sxy - mc.ux * mc.uy;
+            const R Sxz_s = up.x * up.z + mc.sxz - mc.ux * mc.uz;
+            const R Syy_s = up.y * up.y + mc.syy - mc.uy * mc.uy;
+            const R Syz_s = up.y * up.z + mc.syz - mc.uy * mc.uz;
+            const R Szz_s = up.z * up.z + mc.szz - mc.uz * mc.uz;
+            pop = feq<R>(mc.rho, up.x, up.y, up.z, Sxx_s, Sxy_s, Sxz_s, Syy_s, Syz_s, Szz_s, dx, dy, dz, wi);
+            const int ii = inverse(i);
+            const R ex = R(c_cx[ii]), ey = R(c_cy[ii]), ez = R(c_cz[ii]);
+            const R cur_f = feq<R>(mc.rho, mc.ux, mc.uy, mc.uz, mc.sxx, mc.sxy, mc.sxz, mc.syy, mc.syz, mc.szz, ex, ey,
+                                   ez, weight<R>(ii));
+            const R fx = cur_f * (ex - up.x) - pop * (dx - up.x);
+            const R fy = cur_f * (ey - up.y) - pop * (dy - up.y);
+            const R fz = cur_f * (ez - up.z) - pop * (dz - up.z);
+            double* L = acc + 6 * sid;
+            atomicAdd(&L[0], double(fx));
+            atomicAdd(&L[1], double(fy));
+            atomicAdd(&L[2], double(fz));
+            atomicAdd(&L[3], double(ry * fz - rz * fy));
+            atomicAdd(&L[4], double(rz * fx - rx * fz));
+            atomicAdd(&L[5], double(rx * fy - ry * fx));
+          } else {
+            const Mom3<R> m = load_cell<S>(a, N, ((long long)xn * ny + yn) * nz + zn);
+            pop = feq<R>(m.rho, m.ux, m.uy, m.uz, m.sxx, m.sxy, m.sxz, m.syy, m.syz, m.szz, dx, dy, dz, wi);
+            if (pop < R(0)) pop = R(0);
+          }
+        }
+        // moments in the reference's order (528-562)
+        rho_acc = rho_acc + pop;
+        if (ix > 0) { uxp = uxp + pop; pixx = pixx + pop; }
+        else if (ix < 0) { uxm = uxm + pop; pixx = pixx + pop; }
+        if (iy > 0) { uyp = uyp + pop; piyy = piyy + pop; }
+        else if (iy < 0) { uym = uym + pop; piyy = piyy + pop; }
+        if (iz > 0) { uzp = uzp + pop; pizz = pizz + pop; }
+        else if (iz < 0) { uzm = uzm + pop; pizz = pizz + pop; }
+        const int dxy = ix * iy, dxz = ix * iz, dyz = iy * iz;
+        if (dxy > 0) pixy_p = pixy_p + pop;
+        else if (dxy < 0) pixy_m = pixy_m + pop;
+        if (dxz > 0) pixz_p = pixz_p + pop;
+        else if (dxz < 0) pixz_m = pixz_m + pop;
+        if (dyz > 0) piyz_p = piyz_p + pop;
+        else if (dyz < 0) piyz_m = piyz_m + pop;
+      }
+      // regularised collision (564-604)
+      const R Fx = a.w.force ? R(a.w.force[c]) : R(0);
+      const R Fy = a.w.force ? R(a.w.force[N + c]) : R(0);
+      const R Fz = a.w.force ? R(a.w.force[2 * N + c]) : R(0);
+      const R rho = rho_acc;
+      const R invRho = R(1) / rho;
+      const R ux = (uxp - uxm + R(0.5) * Fx) * invRho;
+      const R uy = (uyp - uym + R(0.5) * Fy) * invRho;
+      const R uz = (uzp - uzm + R(0.5) * Fz) * invRho;
+      R pixy = pixy_p - pixy_m, pixz = pixz_p - pixz_m, piyz = piyz_p - piyz_m;
+      const R omega = R(1) / (R(a.vis_shear) * R(3) + R(0.5));
+      const R pixx_part = (R(2) * pixx - piyy - pizz) / R(3);
+      const R piyy_part = (R(2) * piyy - pixx - pizz) / R(3);
+      const R pizz_part = (R(2) * pizz - pixx - piyy) / R(3);
+      const R RU2 = rho * ux * ux, RV2 = rho * uy * uy, RW2 = rho * uz * uz;
+      const R RUVW2 = (RU2 + RV2 + RW2) / R(3);
+      const R o1 = R(1) - omega;
+      const R qxx = rho / R(3) + pixx_part * o1 + RUVW2 + (R(2) * RU2 * omega) / R(3) - (RV2 * omega) / R(3) -
+                    (RW2 * omega) / R(3) + Fx * ux;
+      const R qyy = rho / R(3) + piyy_part * o1 + RUVW2 - (RU2 * omega) / R(3) + (R(2) * RV2 * omega) / R(3) -
+                    (RW2 * omega) / R(3) + Fy * uy;
+      const R qzz = rho / R(3) + pizz_part * o1 + RUVW2 - (RU2 * omega) / R(3) - (RV2 * omega) / R(3) +
+                    (R(2) * RW2 * omega) / R(3) + Fz * uz;
+      pixy = pixy - pixy * omega + ux * uy * rho * omega + (Fy * ux + Fx * uy) / R(2);
+      pixz = pixz - pixz * omega + ux * uz * rho * omega + (Fz * ux + Fx * uz) / R(2);
+      piyz = piyz - piyz * omega + uy * uz * rho * omega + (Fz * uy + Fy * uz) / R(2);
+      const R cs2 = R(1.0 / 3.0);
+      Mom3<R> m;
+      m.rho = rho;
+      m.drho = rho - R(1);
+      m.ux = ux + Fx * invRho / R(2);
+      m.uy = uy + Fy * invRho / R(2);
+      m.uz = uz + Fz * invRho / R(2);
+      m.sxx = qxx * invRho - cs2;
+      m.syy = qyy * invRho - cs2;
+      m.szz = qzz * invRho - cs2;
+      m.sxy = pixy * invRho;
+      m.sxz = pixz * invRho;
+      m.syz = piyz * invRho;
+      R raw[10];
+      encode3<S>(m, a.sc, raw);
+      T* post = static_cast<T*>(a.w.post);
+#pragma unroll
+      for (int k = 0; k < 10; ++k) post[k * N + c] = S::from_r(raw[k]);
+    }
+  }
+  if (!__syncthreads_or(any)) return;
+  for (int k = threadIdx.x; k < 6 * n; k += blockDim.x)
+    if (acc[k] != 0.0) atomicAdd(&s.loads64[k], acc[k]);
+}
+
+// solid_force / solid_torque <- binary32 copies of the binary64 sums.
+__global__ void loads_out_kernel(hl_solids3d s) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= s.n_objects) return;
+  for (int j = 0; j < 3; ++j) {
+    if (s.force) s.force[3 * k + j] = float(s.loads64[6 * k + j]);
+    if (s.torque) s.torque[3 * k + j] = float(s.loads64[6 * k + 3 + j]);
+  }
+}
+
+template <class S> int launch(const hl_world3d* w, double vis, const hl_solids3d* s, cudaStream_t st) {
+  Args a;
+  a.w = *w;
+  a.vis_shear = vis;
+  a.s = *s;
+  a.sc = make_scale(w->storage);
+  // cells within r = max_bound_radius + 2 of a point lie in floor(p - r) .. floor(p - r) + side - 1
+  a.box_side = int(ceilf(2.f * (s->max_bound_radius + 2.f))) + 2;
+  const long long cells = (long long)a.box_side * a.box_side * a.box_side;
+  const dim3 grid(unsigned((cells + BLOCK - 1) / BLOCK), unsigned(s->n_objects));
+  band_kernel<S><<<grid, BLOCK, 0, st>>>(a);
+  HL_LAUNCH_CHECK("d3q27 solid links (band)");
+  loads_out_kernel<<<(s->n_objects + 63) / 64, 64, 0, st>>>(*s);
+  HL_LAUNCH_CHECK("d3q27 solid links (loads)");
+  return HL_OK;
+}
+
+}  // namespace d3s
+}  // namespace hl
+
+using namespace hl;
+
+extern "C" int hl_d3q27_solid_links(const hl_world3d* w, double vis_shear, const hl_solids3d* s, hl_stream stream) {
+  HL_CHECK_ARG(w != nullptr && s != nullptr, "d3q27 solid links: world or solids is NULL");
+  HL_CHECK_ARG(w->nx >= 1 && w->ny >= 1 && w->nz >= 1, "d3q27 solid links: bad dims %d x %d x %d", w->nx, w->ny, w->nz);
+  HL_CHECK_ARG(w->cur != nullptr && w->post != nullptr && w->cur != w->post, "d3q27 solid links: cur/post must be distinct");
+  HL_CHECK_ARG(vis_shear > 0.0, "d3q27 solid links: viscosity must be positive");
+  HL_CHECK_ARG(s->n_objects >= 0 && s->n_objects <= d3s::MAX_SOLIDS, "d3q27 solid links: %d solids (at most %d)",
+               s->n_objects, d3s::MAX_SOLIDS);
+  if (s->n_objects == 0) return HL_OK;
+  HL_CHECK_ARG(s->tri_offset && s->tris && s->transforms && s->transforms_last && s->initialized && s->scale_sizes &&
+                   s->position && s->bound_radius && s->linear_v && s->angle_v && s->loads64,
+               "d3q27 solid links: a solid field is NULL");
+  HL_CHECK_ARG(std::isfinite(s->max_bound_radius) && s->max_bound_radius >= 0.f && s->max_bound_radius < 512.f,
+               "d3q27 solid links: max_bound_radius %g out of range", double(s->max_bound_radius));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(s->loads64, 0, sizeof(double) * 6 * size_t(s->n_objects), st);
+  if (e != cudaSuccess) return cuda_status(e, "d3q27 solid links: zero loads");
+  switch (w->storage.dtype) {
+    case HL_F32: return d3s::launch<StoreF32>(w, vis_shear, s, st);
+    case HL_F16: return d3s::launch<StoreF16>(w, vis_shear, s, st);
+    case HL_BF16: return d3s::launch<StoreBF16>(w, vis_shear, s, st);
+    case HL_F64: return d3s::launch<StoreF64>(w, vis_shear, s, st);
+  }
+  set_error("d3q27 solid links: storage dtype %d not supported", int(w->storage.dtype));
+  return HL_ERR_UNSUPPORTED;
+}

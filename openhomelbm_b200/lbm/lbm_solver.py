@@ -35,6 +35,19 @@ class LBM_Solver:
             f.Initialize(nx, ny, n_objects=solid_num, device=self.device, storage=storage, u_scale=u_scale,
                          s_scale=s_scale, periodic=periodic)
             self.flows.append(f)
+        # per-solid poses and loads of all worlds in batched tensors; each world's HomeFlow
+        # fields are views of its row, so the coupling kernels serve every world in one launch
+        W, n = self.nworld, self.solid_num
+        f32 = dict(dtype=torch.float32, device=self.device)
+        self.solid_position_all = torch.zeros((W, n, 2), **f32)
+        self.solid_angle_all = torch.zeros((W, n), **f32)
+        self.solid_loads_all = torch.zeros((W, 3, n), **f32)  # solid_forcex, solid_forcey, torque
+        for w, f in enumerate(self.flows):
+            f.solid_position = self.solid_position_all[w]
+            f.solid_angle = self.solid_angle_all[w]
+            f.solid_forcex = self.solid_loads_all[w, 0]
+            f.solid_forcey = self.solid_loads_all[w, 1]
+            f.torque = self.solid_loads_all[w, 2]
         self.total_steps = 500000
         self.per_frame_t = 500
         L = _lib.lib()

@@ -1,7 +1,8 @@
 """D3Q27 solver (drop-in for envs/lbm3d/lbm_solver_3d.py's LBM_Solver3D).
 
 ``step()`` advances every world by one step with the CUDA kernels of libhomelbm:
-stream-collide (stream_and_collide_3d), outer boundaries (apply_bc_3d) and the buffer
+stream-collide (stream_and_collide_3d), the cut links and loads of the immersed meshes
+(its narrow band and init_force_3d_batch), outer boundaries (apply_bc_3d) and the buffer
 swap (Swap_Mom_3D). As in the reference (lbm_solver_3d.py:102-127) the first call
 captures the step into a CUDA graph and later calls replay it; the graph is captured
 once per buffer parity and again whenever viscosity, boundary conditions or buffers
@@ -9,7 +10,7 @@ change (the reference invalidates its graph the same way, karman_lbm_env_3d.py:2
 """
 from __future__ import annotations
 
-from typing import Any, Optional, Sequence, Tuple
+from typing import Any, Dict, Optional, Sequence, Tuple
 
 import numpy as np
 import torch
@@ -57,6 +58,12 @@ class LBM_Solver3D:
         self.health = torch.zeros(self.nworld, dtype=torch.int32, device=self.device)
         self.diagnostics = False
         self.meshes = [None] * self.solid_num
+        self._mesh_tris = [None] * self.solid_num
+        self._tris = torch.zeros((1, 3, 3), dtype=torch.float32, device=self.device)
+        self._tri_offset = torch.zeros(self.solid_num + 1, dtype=torch.int32, device=self.device)
+        self._max_bound_radius = 0.0
+        self._solid_version = 0
+        self._batch_solid_state()
         self.mujoco_mappings = {}
         self.mujoco_origins_wp = None
         self.lbm_origins_wp = None
@@ -64,9 +71,66 @@ class LBM_Solver3D:
         self.solid_ids_wp = None
         self.solid_id_to_index = {}
 
+    def _batch_solid_state(self) -> None:
+        """Per-solid state of all worlds in batched tensors [nworld][n][...]; each world's
+        HomeFlow3D fields are views of its row, so the coupling kernels address every world in
+        one launch (the reference launches them over (nworld, n_solids) the same way)."""
+        W, n, dev = self.nworld, self.solid_num, self.device
+        f32 = dict(dtype=torch.float32, device=dev)
+        self.solid_position_all = torch.zeros((W, n, 3), **f32)
+        self.solid_quaternion_all = torch.zeros((W, n, 4), **f32)
+        self.mesh_transforms_all = torch.zeros((W, n, 7), **f32)
+        self.mesh_transforms_last_all = torch.zeros((W, n, 7), **f32)
+        self.mesh_transforms_initialized_all = torch.zeros((W, n), dtype=torch.int32, device=dev)
+        self.mesh_scale_sizes_all = torch.ones((W, n, 3), **f32)
+        self.solid_bound_radius_all = torch.zeros((W, n), **f32)
+        self.linear_v_all = torch.zeros((W, n, 3), **f32)
+        self.angle_v_all = torch.zeros((W, n, 3), **f32)
+        self.solid_force_all = torch.zeros((W, n, 3), **f32)
+        self.solid_torque_all = torch.zeros((W, n, 3), **f32)
+        self.loads64_all = torch.zeros((W, n, 6), dtype=torch.float64, device=dev)
+        for w, f in enumerate(self.flows):
+            f.solid_position = self.solid_position_all[w]
+            f.solid_quaternion = self.solid_quaternion_all[w]
+            f.mesh_transforms = self.mesh_transforms_all[w]
+            f.mesh_transforms_last = self.mesh_transforms_last_all[w]
+            f.mesh_transforms_initialized = self.mesh_transforms_initialized_all[w]
+            f.mesh_scale_sizes = self.mesh_scale_sizes_all[w]
+            f.solid_bound_radius = self.solid_bound_radius_all[w]
+            f.linear_v = self.linear_v_all[w]
+            f.angle_v = self.angle_v_all[w]
+            f.solid_force = self.solid_force_all[w]
+            f.solid_torque = self.solid_torque_all[w]
+            f.loads64 = self.loads64_all[w]
+
+    def _solids_struct(self, k: int) -> _lib.hl_solids3d:
+        f = self.flows[k]
+        s = _lib.hl_solids3d()
+        s.n_objects = self.solid_num
+        s.max_bound_radius = float(self._max_bound_radius)
+        s.tri_offset = self._tri_offset.data_ptr()
+        s.tris = self._tris.data_ptr()
+        for name in ("transforms", "transforms_last"):
+            setattr(s, name, getattr(f, "mesh_" + name).data_ptr())
+        s.initialized = f.mesh_transforms_initialized.data_ptr()
+        s.scale_sizes = f.mesh_scale_sizes.data_ptr()
+        s.position = f.solid_position.data_ptr()
+        s.bound_radius = f.solid_bound_radius.data_ptr()
+        s.linear_v = f.linear_v.data_ptr()
+        s.angle_v = f.angle_v.data_ptr()
+        s.loads64 = f.loads64.data_ptr()
+        s.force = f.solid_force.data_ptr()
+        s.torque = f.solid_torque.data_ptr()
+        return s
+
+    @property
+    def has_meshes(self) -> bool:
+        return any(t is not None and len(t) for t in self._mesh_tris)
+
     # ------------------------------------------------------------------ stepping
     def _launch(self, parity: int, stream) -> None:
         L = _lib.lib()
+        meshes = self.has_meshes
         for k, f in enumerate(self.flows):
             w = f.world_struct(parity)
             diag = None
@@ -74,13 +138,17 @@ class LBM_Solver3D:
                 diag = _lib.hl_diag(self._diag_scratch[k].data_ptr(), self._diag_scratch[k].numel(),
                                     self.mass[k:k + 1].data_ptr(), self.health[k:k + 1].data_ptr())
             _lib.check(L.hl_d3q27_stream_collide(w, float(f.vis_shear), diag, stream), "stream_and_collide_3d")
+            if meshes:
+                _lib.check(L.hl_d3q27_solid_links(w, float(f.vis_shear), self._solids_struct(k), stream),
+                           "stream_and_collide_3d (cut links)")
             if not f.periodic:
                 _lib.check(L.hl_d3q27_apply_bc(w, f.bc_struct(), _lib.ptr(self._bc_scratch[k]), stream),
                            "apply_bc_3d")
 
     def _key(self):
         return tuple((float(f.vis_shear), tuple(map(int, f.bc_type)), f.bc_value.tobytes(), f.use_force,
-                      tuple(m.data_ptr() for m in f.moments)) for f in self.flows) + (self.diagnostics,)
+                      tuple(m.data_ptr() for m in f.moments)) for f in self.flows) + (self.diagnostics,
+                                                                                       self._solid_version)
 
     def step(self) -> None:
         """Advance every world by one LBM step (reference: LBM_Solver3D.step, 88-127)."""
@@ -149,6 +217,118 @@ class LBM_Solver3D:
                                                _lib.ptr(f.moments[0]), _lib.ptr(f.moments[1]), _lib.ptr(f.force),
                                                0.0, 0.0, 0.0, _lib.stream_ptr()), "ResetSingleWorldFlow3D")
             f.mesh_transforms_initialized.zero_()
+
+    # ------------------------------------------------------------------ solids
+    def create_solid_from_mesh(self, solid_id: int, mesh: Any, lbm_position: Optional[Tuple[float, float, float]] = None,
+                               lbm_scale: float = 0.15, init_quaternion: Tuple[float, float, float, float] = (1, 0, 0, 0),
+                               mujoco_origin: Optional[np.ndarray] = None) -> Dict[str, Any]:
+        """The same triangle-mesh solid in every world (lbm_solver_3d.py:128-226).
+
+        ``mesh`` is anything with ``vertices`` (V, 3) and ``faces`` (F, 3) in the body frame
+        (a trimesh.Trimesh, or a (vertices, faces) pair). The vertices are scaled by
+        ``lbm_scale * nx`` and not recentred; ``bound_radius`` is the largest scaled vertex
+        norm. The solid starts at ``lbm_position`` (default: the domain centre) with
+        ``init_quaternion`` (w, x, y, z) and zero wall velocity.
+        """
+        sid = int(solid_id)
+        if not 0 <= sid < self.solid_num:
+            raise ValueError(f"solid_id {solid_id} out of range [0, {self.solid_num})")
+        if isinstance(mesh, (tuple, list)):
+            verts, faces = np.asarray(mesh[0], np.float64), np.asarray(mesh[1], np.int64)
+            mesh_local = (verts.copy(), faces.copy())
+        else:
+            verts, faces = np.asarray(mesh.vertices, np.float64), np.asarray(mesh.faces, np.int64)
+            mesh_local = mesh.copy() if hasattr(mesh, "copy") else mesh
+        if verts.ndim != 2 or verts.shape[1] != 3 or (faces.size and (faces.ndim != 2 or faces.shape[1] != 3)):
+            raise ValueError("mesh needs vertices (V, 3) and faces (F, 3)")
+        lbm_scale_actual = float(lbm_scale) * self.nx
+        scaled_vertices = verts * lbm_scale_actual
+        if lbm_position is None:
+            lbm_position = (self.nx * 0.5, self.ny * 0.5, self.nz * 0.5)
+        self.meshes[sid] = mesh_local
+        vertices = np.array(scaled_vertices, dtype=np.float32)
+        bound_radius = float(np.linalg.norm(vertices, axis=1).max()) if len(vertices) else 0.0
+        self._mesh_tris[sid] = vertices[faces] if faces.size else np.zeros((0, 3, 3), np.float32)
+        self._upload_meshes()
+        for f in self.flows:
+            f.mesh_ids[sid] = sid + 1
+            f.mesh_scale_sizes[sid] = 1.0
+            f.solid_position[sid] = torch.tensor(np.asarray(lbm_position, np.float32), device=self.device)
+            f.solid_quaternion[sid] = torch.tensor(np.asarray(init_quaternion, np.float32), device=self.device)
+            f.solid_bound_radius[sid] = bound_radius
+            self._update_mesh_transform(f, sid)
+        if mujoco_origin is None:
+            mujoco_origin = np.zeros(3, dtype=np.float32)
+        self.mujoco_mappings[sid] = {"mujoco_origin": np.array(mujoco_origin, dtype=np.float32),
+                                     "lbm_origin": np.array(lbm_position, dtype=np.float32),
+                                     "scale": lbm_scale_actual}
+        return {"mesh": mesh_local, "vertices": scaled_vertices, "scale": lbm_scale_actual,
+                "lbm_position": lbm_position, "quaternion": init_quaternion}
+
+    def _upload_meshes(self) -> None:
+        tris = [t if t is not None else np.zeros((0, 3, 3), np.float32) for t in self._mesh_tris]
+        counts = [len(t) for t in tris]
+        offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+        allt = np.concatenate(tris) if sum(counts) else np.zeros((1, 3, 3), np.float32)
+        self._tris = torch.tensor(np.ascontiguousarray(allt, np.float32), device=self.device)
+        self._tri_offset = torch.tensor(offs, device=self.device)
+        radii = [float(np.linalg.norm(t.reshape(-1, 3), axis=1).max()) for t in tris if len(t)]
+        self._max_bound_radius = max(radii) if radii else 0.0
+        self._solid_version += 1
+
+    def _update_mesh_transform(self, flow: HomeFlow3D, solid_id: int) -> None:
+        """New mesh transform from solid_position / solid_quaternion (lbm_solver_3d.py:228-254):
+        the first time both transforms are set (zero wall velocity), afterwards the current one
+        becomes the last."""
+        pos = flow.solid_position[solid_id].detach().cpu().numpy()
+        q = flow.solid_quaternion[solid_id].detach().cpu().numpy()  # w, x, y, z
+        new = torch.tensor([pos[0], pos[1], pos[2], q[1], q[2], q[3], q[0]], dtype=torch.float32, device=self.device)
+        if int(flow.mesh_transforms_initialized[solid_id]) == 0:
+            flow.mesh_transforms[solid_id] = new
+            flow.mesh_transforms_last[solid_id] = new
+            flow.mesh_transforms_initialized[solid_id] = 1
+        else:
+            flow.mesh_transforms_last[solid_id] = flow.mesh_transforms[solid_id].clone()
+            flow.mesh_transforms[solid_id] = new
+
+    def update_solids_batch(self, world_idx: int, solid_ids: Sequence[int], positions: np.ndarray,
+                            quaternions: np.ndarray) -> None:
+        """Poses of several solids of one world from MuJoCo positions (N, 3) and quaternions
+        (N, 4) in (w, x, y, z) order (lbm_solver_3d.py:256-292)."""
+        flow = self.flows[world_idx]
+        positions = np.asarray(positions, np.float32)
+        quaternions = np.asarray(quaternions, np.float32)
+        for i, sid in enumerate(solid_ids):
+            if sid in self.mujoco_mappings:
+                m = self.mujoco_mappings[sid]
+                lbm_pos = (positions[i] - m["mujoco_origin"]) * np.float32(m["scale"]) + m["lbm_origin"]
+            else:
+                lbm_pos = positions[i]
+            flow.solid_position[sid] = torch.tensor(np.asarray(lbm_pos, np.float32), device=self.device)
+            flow.solid_quaternion[sid] = torch.tensor(quaternions[i], device=self.device)
+        for sid in solid_ids:
+            self._update_mesh_transform(flow, sid)
+
+    def get_forces_and_torques(self, world_idx: int, solid_ids: Optional[Sequence[int]] = None
+                               ) -> Tuple[np.ndarray, np.ndarray]:
+        """Forces and torques (N, 3) of a world's solids, divided by the mapping scale and its
+        square where a MuJoCo mapping exists (lbm_solver_3d.py:294-333)."""
+        if solid_ids is None:
+            solid_ids = list(range(self.solid_num))
+        flow = self.flows[world_idx]
+        sf = flow.solid_force.detach().cpu().numpy()
+        st = flow.solid_torque.detach().cpu().numpy()
+        forces = np.zeros((len(solid_ids), 3), np.float32)
+        torques = np.zeros((len(solid_ids), 3), np.float32)
+        for i, sid in enumerate(solid_ids):
+            if sid in self.mujoco_mappings:
+                scale = self.mujoco_mappings[sid]["scale"]
+                forces[i] = sf[sid] / scale
+                torques[i] = st[sid] / (scale * scale)
+            else:
+                forces[i] = sf[sid]
+                torques[i] = st[sid]
+        return forces, torques
 
     def finalize_mappings(self, solid_ids: Sequence[int]) -> None:
         """Coordinate-mapping arrays for batch coupling (lbm_solver_3d.py:387-418)."""
