@@ -305,6 +305,142 @@ def run_ours(args, rank, world, dist):
     return out
 
 
+# ----------------------------------------------------------------------------- precision form
+def tgv_diagnostics(f, n):
+    """Kinetic energy 1/2 <rho |u|^2> and enstrophy 1/2 <|curl u|^2> (periodic central
+    differences, unit lattice spacing) of a world, in binary64."""
+    import torch
+
+    m = f.decoded().double()
+    rho, u = m[0], m[1:4]
+    ke = 0.5 * float((rho * (u * u).sum(0)).mean())
+
+    def d(a, axis):
+        return 0.5 * (torch.roll(a, -1, axis) - torch.roll(a, 1, axis))
+
+    wx = d(u[2], 1) - d(u[1], 2)
+    wy = d(u[0], 2) - d(u[2], 0)
+    wz = d(u[1], 0) - d(u[0], 1)
+    ens = 0.5 * float((wx * wx + wy * wy + wz * wz).mean())
+    return ke, ens
+
+
+def run_precision(args):
+    """The precision form: the Taylor-Green vortex with float64 (the accuracy oracle, same
+    kernels in binary64), float32, float16 and bfloat16 storage. Each run records kinetic
+    energy and enstrophy every 10 steps and the binary64 mass sum every step; the reduced
+    forms report their velocity L2 error against the float64 run and their MLUPS against
+    the float32 run (timed separately, diagnostics off)."""
+    import torch
+
+    from openhomelbm_b200.lbm3d import LBM_Solver3D
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n, steps, u0 = args.n, args.steps, 0.04
+    vis = u0 * (n / (2 * np.pi)) / 1600.0
+    cells = n ** 3
+    every = 10
+    res, u_ref = {}, None
+    for storage in ("float64", "float32", "float16", "bfloat16"):
+        s = LBM_Solver3D(n, n, n, solid_num=1, periodic=True, storage=storage, device=dev, u_scale=u0,
+                         s_scale=u0 * u0)
+        s.set_viscosity(vis)
+        s.init_tgv(u0)
+        f = s.flows[0]
+        s.diagnostics = True
+        ke, ens, mass = [], [], torch.zeros(steps, dtype=torch.float64, device=dev)
+        k0, e0 = tgv_diagnostics(f, n)
+        ke.append(k0)
+        ens.append(e0)
+        for k in range(steps):
+            s.step()
+            mass[k] = s.mass[0]
+            if (k + 1) % every == 0:
+                kk, ee = tgv_diagnostics(f, n)
+                ke.append(kk)
+                ens.append(ee)
+        s.diagnostics = False
+        u = f.decoded()[1:4].double()
+        rec = {"ke_every_10": [round(x, 12) for x in ke], "enstrophy_every_10": [round(x, 12) for x in ens],
+               "mass_first": float(mass[0]), "mass_last": float(mass[-1]),
+               "mass_rel_drift": float((mass[-1] - mass[0]) / mass[0]), "health": int(s.health[0])}
+        if u_ref is None:
+            u_ref = u.clone()
+        else:
+            rec["u_l2_vs_float64"] = float(torch.linalg.vector_norm(u - u_ref) / torch.linalg.vector_norm(u_ref))
+        del u
+        # throughput, diagnostics off
+        for _ in range(3):
+            s.step()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        timed = min(steps, 200)
+        a.record()
+        for _ in range(timed):
+            s.step()
+        b.record()
+        torch.cuda.synchronize()
+        rec["mlups"] = cells * timed / (a.elapsed_time(b) / 1e3) / 1e6
+        res[storage] = rec
+        del s, f
+        torch.cuda.empty_cache()
+    f32 = res["float32"]["mlups"]
+    for st in ("float16", "bfloat16"):
+        res[st]["mlups_vs_float32"] = res[st]["mlups"] / f32
+    return {"metric": f"D3Q27 velocity L2 vs float64 (Taylor-Green {n}^3, {steps} steps, reduced storage)",
+            "value": res["float16"]["u_l2_vs_float64"], "unit": "relative L2", "higher_is_better": False,
+            "n_gpus": 1, "steps": steps, "workload": "precision", "dtype": "f32 arithmetic",
+            "data": "synthetic (Taylor-Green initial state)",
+            "config": {"workload": f"D3Q27 Taylor-Green vortex {n}^3 periodic; float64 / float32 / float16 / bfloat16 "
+                                   "storage (rho - 1, u / u0, (S - u u) / u0^2)", "u0": u0, "Re": 1600,
+                       "vis_shear": vis, "diagnostics_every": every},
+            "results": res}
+
+
+# ----------------------------------------------------------------------------- serving form
+def run_serve(args):
+    """The serving form: Poisson arrivals of mesh-coupled D3Q27 domains (sides log-uniform in
+    64-192, rounded to multiples of 32; a 5-segment swimmer of 1800 triangles; 8 LBM substeps
+    per control step, 100 control steps per request). The served engine (float16 storage,
+    resident fields, one CUDA graph per domain control step, concurrent domains) against the
+    plain solver one request at a time (float32), on the same request set."""
+    import torch
+
+    from openhomelbm_b200 import serving
+
+    torch.cuda.set_device(0)
+    reqs = serving.poisson_requests(args.requests, args.rate, seed=7, control_steps=args.control_steps)
+    warm = [serving.Request(10 ** 6, 64, 1, 0.0, control_steps=2, substeps=8)]
+    serving.run_plain(warm)
+    serving.ServeEngine(storage="float16", max_active=1).run(warm, realtime=False)
+    torch.cuda.synchronize()
+    plain = serving.run_plain(reqs, storage="float32")
+    served = serving.ServeEngine(storage="float16", max_active=args.slots, budget_bytes=150e9).run(reqs)
+    # agreement of the served float16 loads with the plain float32 loads, request by request
+    errs = []
+    for r in reqs:
+        a, b = served.results[r.rid].astype(np.float64), plain.results[r.rid].astype(np.float64)
+        errs.append(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)))
+    cells = sum(r.side ** 3 * r.control_steps * r.substeps for r in reqs)
+    sides = [r.side for r in reqs]
+    return {"metric": "served env-steps/s (D3Q27 mesh-coupled domains, float16 storage, continuous batching)",
+            "value": served.env_steps_per_s, "unit": "env-steps/s", "higher_is_better": True, "n_gpus": 1,
+            "workload": "serve", "dtype": "f32 arithmetic, f16 storage", "data": "synthetic (seeded Poisson requests)",
+            "vs_plain": served.env_steps_per_s / plain.env_steps_per_s,
+            "served": {"env_steps_per_s": served.env_steps_per_s, "p50_ms": served.pct(50) * 1e3,
+                       "p99_ms": served.pct(99) * 1e3, "p99_over_p50": served.pct(99) / served.pct(50),
+                       "wall_s": served.wall_s, "max_active": served.max_active,
+                       "mlups": cells / served.wall_s / 1e6},
+            "plain": {"env_steps_per_s": plain.env_steps_per_s, "p50_ms": plain.pct(50) * 1e3,
+                      "p99_ms": plain.pct(99) * 1e3, "wall_s": plain.wall_s, "mlups": cells / plain.wall_s / 1e6},
+            "loads_rel_l2_f16_vs_plain_f32": {"median": float(np.median(errs)), "max": float(np.max(errs))},
+            "config": {"requests": len(reqs), "rate_per_s": args.rate, "control_steps": args.control_steps,
+                       "substeps": 8, "slots": args.slots, "hbm_budget_gb": 150,
+                       "sides": {str(k): sides.count(k) for k in sorted(set(sides))},
+                       "triangles_per_body": 1800, "segments": serving.SEGMENTS}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -319,6 +455,13 @@ def main():
     ap.add_argument("--kernel", type=int, default=0, help="0 auto, 1 async-copy kernel, 2 TMA kernel")
     ap.add_argument("--chunks", type=int, default=0, help="x split per tile column (0 automatic)")
     ap.add_argument("--stages", type=int, default=0, help="TMA pipeline stages (0 automatic)")
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "precision", "serve"],
+                    help="tgv: the headline throughput line; precision: float64/32/16/bf16 accuracy form; "
+                         "serve: served vs plain mesh-coupled domains")
+    ap.add_argument("--requests", type=int, default=48, help="serve: number of requests")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate (requests/s)")
+    ap.add_argument("--control-steps", type=int, default=100, help="serve: control steps per request")
+    ap.add_argument("--slots", type=int, default=32, help="serve: concurrently resident domains")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -337,6 +480,10 @@ def main():
     try:
         if args.impl == "reference":
             out = run_reference(args, rank, world)
+        elif args.workload == "precision":
+            out = run_precision(args) if rank == 0 else None
+        elif args.workload == "serve":
+            out = run_serve(args) if rank == 0 else None
         else:
             out = run_ours(args, rank, world, dist)
         if rank == 0 and out is not None:

@@ -182,6 +182,19 @@ typedef struct {
   double* loads64;           /* [n][6] scratch: force then torque summed in binary64 */
   float* force;              /* [n][3] solid_force (out) */
   float* torque;             /* [n][3] solid_torque (out) */
+  /* Optional triangle bins (NULL: every link ray tests all triangles of the solid). Per solid
+   * a uniform grid in its body frame; bin (i, j, k) lists the triangles whose bounding box,
+   * widened by at least sqrt(3) (the longest link), meets the bin, so a ray starting in the
+   * bin finds every hit with t <= 1 among them (same closest hit as testing all). Used where
+   * mesh_scale_sizes is (1, 1, 1); other solids fall back to all triangles. */
+  const float* bin_box;      /* [n][4] grid origin x, y, z and bin edge */
+  const int32_t* bin_dims;   /* [n][4] bins along x, y, z (0: no grid) and the solid's first bin */
+  const int32_t* bin_start;  /* [bins + n] start of each bin's list in bin_tris (CSR per solid) */
+  const int32_t* bin_tris;   /* triangle indices, relative to the solid's first triangle */
+  /* Scratch of hl_d3q27_solid_links_work_ints() int32 (NULL: the single-pass kernel): the
+   * list of cells that can have a cut link, so that the cut-cell work is spread evenly over
+   * the GPU instead of staying with the warps whose cells happen to lie near the surface. */
+  int32_t* work;
 } hl_solids3d;
 
 /* The solid part of one stream_and_collide_3d step (envs/lbm3d/lbm_func_3d.py:364-604) and
@@ -194,6 +207,10 @@ typedef struct {
  * (525-526); the momentum exchange and its torque about solid_position (490-511) are summed
  * per solid in binary64 and copied to force / torque in binary32. */
 HL_API int hl_d3q27_solid_links(const hl_world3d* w, double vis_shear, const hl_solids3d* s, hl_stream stream);
+
+/* int32 entries of the work scratch of hl_solids3d for n_objects solids whose bound_radius is
+ * at most max_bound_radius. */
+HL_API size_t hl_d3q27_solid_links_work_ints(int n_objects, float max_bound_radius);
 
 /* ------------------------------------------------------------------ coupling
  * The MuJoCo-Warp coupling kernels of the environments, over batched per-world arrays:

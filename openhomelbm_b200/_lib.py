@@ -46,7 +46,8 @@ class hl_solids3d(Structure):
                 ("transforms", c_void_p), ("transforms_last", c_void_p), ("initialized", c_void_p),
                 ("scale_sizes", c_void_p), ("position", c_void_p), ("bound_radius", c_void_p),
                 ("linear_v", c_void_p), ("angle_v", c_void_p), ("loads64", c_void_p), ("force", c_void_p),
-                ("torque", c_void_p)]
+                ("torque", c_void_p), ("bin_box", c_void_p), ("bin_dims", c_void_p), ("bin_start", c_void_p),
+                ("bin_tris", c_void_p), ("work", c_void_p)]
 
 
 class hl_world2d(Structure):
@@ -84,6 +85,7 @@ _SIGS = {
     "hl_d3q27_stream_collide_noalloc": ([POINTER(hl_world3d), c_double, c_void_p, c_void_p, c_void_p], c_int),
     "hl_d3q27_bc_scratch_bytes": ([POINTER(hl_world3d)], c_size_t),
     "hl_d3q27_solid_links": ([POINTER(hl_world3d), c_double, POINTER(hl_solids3d), c_void_p], c_int),
+    "hl_d3q27_solid_links_work_ints": ([c_int, c_float], c_size_t),
     "hl_couple_body_states": ([c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int),
     "hl_couple3d_update_solids": ([c_int, c_int, c_int] + [c_void_p] * 12, c_int),
     "hl_couple2d_update_solids": ([c_int, c_int, c_int] + [c_void_p] * 9, c_int),

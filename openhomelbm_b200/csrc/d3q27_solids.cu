@@ -16,8 +16,13 @@
 // written by the plain kernel; both read only the current buffer.
 //
 // Launch: one block row per solid (blockIdx.y), covering that solid's bounding box of the
-// band; a cell near several solids is handled by the lowest-numbered one. Loads are summed
-// per block in shared memory and per solid in binary64 global memory.
+// band; a cell near several solids is handled by the lowest-numbered one. Only cells that can
+// have a cut link are recomputed: with the triangle bins a cell whose bin lists no triangle
+// of any near solid has none (the rays are at most sqrt(3) long), and keeps the plain
+// kernel's result, which is the reference's arithmetic on plain links up to rounding. Each
+// remaining cell is computed by a whole warp, one lane per direction; its moments are warp
+// shuffle sums, and the loads are summed per block in shared memory and per solid in
+// binary64 global memory.
 //
 // Ray-triangle test: Moller & Trumbore, "Fast, minimum storage ray-triangle intersection"
 // (1997), double-sided, closest hit with 0 <= t <= max_t = 2 (the reference's mesh query
@@ -73,13 +78,24 @@ template <class R> __device__ __forceinline__ V3<R> xpoint(const Xf<R>& t, V3<R>
   return {r.x + t.p.x, r.y + t.p.y, r.z + t.p.z};
 }
 
-// Closest double-sided hit 0 <= t <= max_t of the ray o + t d with the triangles.
+// Closest double-sided hit 0 <= t <= max_t of the ray o + t d with the triangles tri[list[k]]
+// (k < ntri; list NULL: tri[k]). The caller keeps a hit only when t <= 1, so a triangle whose
+// bounding box misses the box of the segment t in [0, 1] (widened by 1e-3 against rounding)
+// cannot change the outcome and is skipped before the exact test.
 template <class R>
-__device__ bool ray_mesh(const float* tri, int ntri, V3<R> o, V3<R> d, R max_t, R* t_out) {
+__device__ bool ray_mesh(const float* tri, const int32_t* list, int ntri, V3<R> o, V3<R> d, R max_t, R* t_out) {
   bool hit = false;
   R best = R(0);
+  const float eps = 1e-3f;
+  const float sx0 = float(fmin(o.x, o.x + d.x)) - eps, sx1 = float(fmax(o.x, o.x + d.x)) + eps;
+  const float sy0 = float(fmin(o.y, o.y + d.y)) - eps, sy1 = float(fmax(o.y, o.y + d.y)) + eps;
+  const float sz0 = float(fmin(o.z, o.z + d.z)) - eps, sz1 = float(fmax(o.z, o.z + d.z)) + eps;
   for (int k = 0; k < ntri; ++k) {
-    const float* v = tri + 9 * k;
+    const float* v = tri + 9 * (list ? list[k] : k);
+    if (fmaxf(fmaxf(v[0], v[3]), v[6]) < sx0 || fminf(fminf(v[0], v[3]), v[6]) > sx1 ||
+        fmaxf(fmaxf(v[1], v[4]), v[7]) < sy0 || fminf(fminf(v[1], v[4]), v[7]) > sy1 ||
+        fmaxf(fmaxf(v[2], v[5]), v[8]) < sz0 || fminf(fminf(v[2], v[5]), v[8]) > sz1)
+      continue;
     const R v0x = R(v[0]), v0y = R(v[1]), v0z = R(v[2]);
     const R e1x = R(v[3]) - v0x, e1y = R(v[4]) - v0y, e1z = R(v[5]) - v0z;
     const R e2x = R(v[6]) - v0x, e2y = R(v[7]) - v0y, e2z = R(v[8]) - v0z;
@@ -146,9 +162,204 @@ template <class R> __device__ __forceinline__ int first_near(const hl_solids3d& 
   return -1;
 }
 
-template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __grid_constant__ Args a) {
+// Candidate triangles of solid k for rays starting at the body-frame point lo: the bin's list,
+// or every triangle when the solid has no bins (or a non-unit mesh scale). Returns false when
+// the bin is empty or lo lies outside the grid: no link from there can hit the solid.
+template <class R>
+__device__ __forceinline__ bool candidates(const hl_solids3d& s, int k, int ntri, V3<R> los, R sx, R sy, R sz,
+                                           const int32_t** list, int* ncand) {
+  *list = nullptr;
+  *ncand = ntri;
+  if (s.bin_box == nullptr || s.bin_dims[4 * k] <= 0 || sx != R(1) || sy != R(1) || sz != R(1)) return ntri > 0;
+  const float* bb = s.bin_box + 4 * k;
+  const int* bd = s.bin_dims + 4 * k;
+  const R inv_h = R(1) / R(bb[3]);
+  const R fx = (los.x - R(bb[0])) * inv_h, fy = (los.y - R(bb[1])) * inv_h, fz = (los.z - R(bb[2])) * inv_h;
+  if (!(fx >= R(0) && fy >= R(0) && fz >= R(0) && fx < R(bd[0]) && fy < R(bd[1]) && fz < R(bd[2]))) return false;
+  const int b = bd[3] + (int(fx) * bd[1] + int(fy)) * bd[2] + int(fz);
+  *list = s.bin_tris + s.bin_start[b];
+  *ncand = s.bin_start[b + 1] - s.bin_start[b];
+  return *ncand > 0;
+}
+
+// Whether a link of the cell could be cut: some solid within bound_radius + 2 has candidate
+// triangles for rays from the cell.
+template <class R> __device__ bool may_cut(const hl_solids3d& s, V3<R> cell) {
+  for (int k = 0; k < s.n_objects; ++k) {
+    const int ntri = s.tri_offset[k + 1] - s.tri_offset[k];
+    if (ntri == 0) continue;
+    if (vlen(cell.x - R(s.position[3 * k]), cell.y - R(s.position[3 * k + 1]), cell.z - R(s.position[3 * k + 2])) >
+        R(s.bound_radius[k]) + R(2))
+      continue;
+    const Xf<R> inv = xinv(load_xf<R>(s.transforms + 7 * k));
+    const V3<R> lo = xpoint(inv, cell);
+    const R sx = R(s.scale_sizes[3 * k]), sy = R(s.scale_sizes[3 * k + 1]), sz = R(s.scale_sizes[3 * k + 2]);
+    const int32_t* list;
+    int ncand;
+    if (candidates(s, k, ntri, V3<R>{lo.x / sx, lo.y / sy, lo.z / sz}, sx, sy, sz, &list, &ncand)) return true;
+  }
+  return false;
+}
+
+template <class R> __device__ __forceinline__ R warp_sum(R v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// One near cell with a possible cut link, computed by a whole warp: lane i < 27 rebuilds the
+// population of direction i (a wall population with its momentum exchange if the link is
+// cut, the clamped neighbour population otherwise), the moments are warp sums, and lane 0
+// collides and stores the cell.
+template <class S> __device__ void cut_cell(const Args& a, double* acc, int x, int y, int z) {
   using R = typename S::R;
   using T = typename S::T;
+  const hl_solids3d& s = a.s;
+  const int nx = a.w.nx, ny = a.w.ny, nz = a.w.nz;
+  const long long N = (long long)nx * ny * nz;
+  const long long c = ((long long)x * ny + y) * nz + z;
+  const int i = threadIdx.x & 31;
+  const Mom3<R> mc = load_cell<S>(a, N, c);
+  R pop = R(0);
+  int ix = 0, iy = 0, iz = 0;
+  if (i < 27) {
+    ix = c_cx[i];
+    iy = c_cy[i];
+    iz = c_cz[i];
+    const R dx = R(ix), dy = R(iy), dz = R(iz);
+    const R wi = weight<R>(i);
+    int xn = x - ix, yn = y - iy, zn = z - iz;
+    if (a.w.periodic) {
+      xn = wrap(xn, nx);
+      yn = wrap(yn, ny);
+      zn = wrap(zn, nz);
+    }
+    if (xn >= 0 && xn < nx && yn >= 0 && yn < ny && zn >= 0 && zn < nz) {
+      // get_cutcell_multi_3d: the closest hit in [0, 1] over the solids near the cell
+      R cut = R(-1);
+      int sid = -1;
+      const V3<R> cell{R(x), R(y), R(z)};
+      const V3<R> dir{-dx, -dy, -dz};
+      for (int k = 0; k < s.n_objects; ++k) {
+        const int t0 = s.tri_offset[k], ntri = s.tri_offset[k + 1] - t0;
+        if (ntri == 0) continue;
+        if (vlen(cell.x - R(s.position[3 * k]), cell.y - R(s.position[3 * k + 1]), cell.z - R(s.position[3 * k + 2])) >
+            R(s.bound_radius[k]) + R(2))
+          continue;
+        const Xf<R> inv = xinv(load_xf<R>(s.transforms + 7 * k));
+        const V3<R> lo = xpoint(inv, cell);
+        const V3<R> ld = qrot(inv.qx, inv.qy, inv.qz, inv.qw, dir);
+        const R sx = R(s.scale_sizes[3 * k]), sy = R(s.scale_sizes[3 * k + 1]), sz = R(s.scale_sizes[3 * k + 2]);
+        const V3<R> los{lo.x / sx, lo.y / sy, lo.z / sz};
+        const int32_t* list;
+        int ncand;
+        if (!candidates(s, k, ntri, los, sx, sy, sz, &list, &ncand)) continue;
+        R t;
+        if (ray_mesh<R>(s.tris + 9ll * t0, list, ncand, los, {ld.x / sx, ld.y / sy, ld.z / sz}, R(2), &t)) {
+          if ((cut < R(0) || t < cut) && t >= R(0) && t <= R(1)) {
+            cut = t;
+            sid = k;
+          }
+        }
+      }
+      if (sid >= 0) {
+        const Xf<R> tc = load_xf<R>(s.transforms + 7 * sid);
+        const Xf<R> tl = load_xf<R>(s.transforms_last + 7 * sid);
+        const V3<R> hit{cell.x + dir.x * cut, cell.y + dir.y * cut, cell.z + dir.z * cut};
+        const V3<R> hl = xpoint(xinv(tc), hit);
+        V3<R> up;
+        const R spx = R(s.position[3 * sid]), spy = R(s.position[3 * sid + 1]), spz = R(s.position[3 * sid + 2]);
+        if (s.initialized[sid] > 0) {
+          const V3<R> pc = xpoint(tc, hl), pl = xpoint(tl, hl);
+          up = {pc.x - pl.x, pc.y - pl.y, pc.z - pl.z};
+        } else {
+          const R ax = R(s.angle_v[3 * sid]), ay = R(s.angle_v[3 * sid + 1]), az = R(s.angle_v[3 * sid + 2]);
+          const R rx = hit.x - spx, ry = hit.y - spy, rz = hit.z - spz;
+          up = {R(s.linear_v[3 * sid]) + (ay * rz - az * ry), R(s.linear_v[3 * sid + 1]) + (az * rx - ax * rz),
+                R(s.linear_v[3 * sid + 2]) + (ax * ry - ay * rx)};
+        }
+        const R rx = hit.x - spx, ry = hit.y - spy, rz = hit.z - spz;
+        const R Sxx_s = up.x * up.x + mc.sxx - mc.ux * mc.ux;
+        const R Sxy_s = up.x * up.y + mc.sxy - mc.ux * mc.uy;
+        const R Sxz_s = up.x * up.z + mc.sxz - mc.ux * mc.uz;
+        const R Syy_s = up.y * up.y + mc.syy - mc.uy * mc.uy;
+        const R Syz_s = up.y * up.z + mc.syz - mc.uy * mc.uz;
+        const R Szz_s = up.z * up.z + mc.szz - mc.uz * mc.uz;
+        pop = feq<R>(mc.rho, up.x, up.y, up.z, Sxx_s, Sxy_s, Sxz_s, Syy_s, Syz_s, Szz_s, dx, dy, dz, wi);
+        const int ii = inverse(i);
+        const R ex = R(c_cx[ii]), ey = R(c_cy[ii]), ez = R(c_cz[ii]);
+        const R cur_f = feq<R>(mc.rho, mc.ux, mc.uy, mc.uz, mc.sxx, mc.sxy, mc.sxz, mc.syy, mc.syz, mc.szz, ex, ey, ez,
+                               weight<R>(ii));
+        const R fx = cur_f * (ex - up.x) - pop * (dx - up.x);
+        const R fy = cur_f * (ey - up.y) - pop * (dy - up.y);
+        const R fz = cur_f * (ez - up.z) - pop * (dz - up.z);
+        double* L = acc + 6 * sid;
+        atomicAdd(&L[0], double(fx));
+        atomicAdd(&L[1], double(fy));
+        atomicAdd(&L[2], double(fz));
+        atomicAdd(&L[3], double(ry * fz - rz * fy));
+        atomicAdd(&L[4], double(rz * fx - rx * fz));
+        atomicAdd(&L[5], double(rx * fy - ry * fx));
+      } else {
+        const Mom3<R> m = load_cell<S>(a, N, ((long long)xn * ny + yn) * nz + zn);
+        pop = feq<R>(m.rho, m.ux, m.uy, m.uz, m.sxx, m.sxy, m.sxz, m.syy, m.syz, m.szz, dx, dy, dz, wi);
+        if (pop < R(0)) pop = R(0);
+      }
+    }
+  }
+  // moments (lbm_func_3d.py:528-562) as warp sums: rho, the signed first moments and the
+  // second moments (c_a^2 = |c_a|)
+  const R rho = warp_sum(pop);
+  const R jx = warp_sum(R(ix) * pop), jy = warp_sum(R(iy) * pop), jz = warp_sum(R(iz) * pop);
+  const R pxx = warp_sum(R(ix * ix) * pop), pyy = warp_sum(R(iy * iy) * pop), pzz = warp_sum(R(iz * iz) * pop);
+  R pixy = warp_sum(R(ix * iy) * pop), pixz = warp_sum(R(ix * iz) * pop), piyz = warp_sum(R(iy * iz) * pop);
+  if (i != 0) return;
+  // regularised collision (564-604)
+  const R Fx = a.w.force ? R(a.w.force[c]) : R(0);
+  const R Fy = a.w.force ? R(a.w.force[N + c]) : R(0);
+  const R Fz = a.w.force ? R(a.w.force[2 * N + c]) : R(0);
+  const R invRho = R(1) / rho;
+  const R ux = (jx + R(0.5) * Fx) * invRho;
+  const R uy = (jy + R(0.5) * Fy) * invRho;
+  const R uz = (jz + R(0.5) * Fz) * invRho;
+  const R omega = R(1) / (R(a.vis_shear) * R(3) + R(0.5));
+  const R pixx_part = (R(2) * pxx - pyy - pzz) / R(3);
+  const R piyy_part = (R(2) * pyy - pxx - pzz) / R(3);
+  const R pizz_part = (R(2) * pzz - pxx - pyy) / R(3);
+  const R RU2 = rho * ux * ux, RV2 = rho * uy * uy, RW2 = rho * uz * uz;
+  const R RUVW2 = (RU2 + RV2 + RW2) / R(3);
+  const R o1 = R(1) - omega;
+  const R qxx = rho / R(3) + pixx_part * o1 + RUVW2 + (R(2) * RU2 * omega) / R(3) - (RV2 * omega) / R(3) -
+                (RW2 * omega) / R(3) + Fx * ux;
+  const R qyy = rho / R(3) + piyy_part * o1 + RUVW2 - (RU2 * omega) / R(3) + (R(2) * RV2 * omega) / R(3) -
+                (RW2 * omega) / R(3) + Fy * uy;
+  const R qzz = rho / R(3) + pizz_part * o1 + RUVW2 - (RU2 * omega) / R(3) - (RV2 * omega) / R(3) +
+                (R(2) * RW2 * omega) / R(3) + Fz * uz;
+  pixy = pixy - pixy * omega + ux * uy * rho * omega + (Fy * ux + Fx * uy) / R(2);
+  pixz = pixz - pixz * omega + ux * uz * rho * omega + (Fz * ux + Fx * uz) / R(2);
+  piyz = piyz - piyz * omega + uy * uz * rho * omega + (Fz * uy + Fy * uz) / R(2);
+  const R cs2 = R(1.0 / 3.0);
+  Mom3<R> m;
+  m.rho = rho;
+  m.drho = rho - R(1);
+  m.ux = ux + Fx * invRho / R(2);
+  m.uy = uy + Fy * invRho / R(2);
+  m.uz = uz + Fz * invRho / R(2);
+  m.sxx = qxx * invRho - cs2;
+  m.syy = qyy * invRho - cs2;
+  m.szz = qzz * invRho - cs2;
+  m.sxy = pixy * invRho;
+  m.sxz = pixz * invRho;
+  m.syz = piyz * invRho;
+  R raw[10];
+  encode3<S>(m, a.sc, raw);
+  T* post = static_cast<T*>(a.w.post);
+#pragma unroll
+  for (int k = 0; k < 10; ++k) post[k * N + c] = S::from_r(raw[k]);
+}
+
+template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __grid_constant__ Args a) {
+  using R = typename S::R;
   __shared__ double acc[MAX_SOLIDS * 6];
   const hl_solids3d& s = a.s;
   const int n = s.n_objects;
@@ -157,167 +368,91 @@ template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __
 
   const int k0 = blockIdx.y;
   const int nx = a.w.nx, ny = a.w.ny, nz = a.w.nz;
-  const long long N = (long long)nx * ny * nz;
-  bool any = false;
   // bounding box of solid k0's band, clipped to the grid
   const float px = s.position[3 * k0], py = s.position[3 * k0 + 1], pz = s.position[3 * k0 + 2];
   const float r = s.bound_radius[k0] + 2.f;
   const int side = a.box_side;
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  // 1. each lane classifies its cell: fluid, in solid k0's band (and in no lower solid's), and
+  //    with candidate triangles for its rays
+  int x = 0, y = 0, z = 0;
+  bool flagged = false;
   if (s.tri_offset[k0 + 1] > s.tri_offset[k0] && isfinite(px) && isfinite(py) && isfinite(pz) && isfinite(r) &&
       idx < (long long)side * side * side) {
-    const int bx = int(floorf(px - r)), by = int(floorf(py - r)), bz = int(floorf(pz - r));
-    const int x = bx + int(idx / ((long long)side * side)), y = by + int((idx / side) % side), z = bz + int(idx % side);
+    x = int(floorf(px - r)) + int(idx / ((long long)side * side));
+    y = int(floorf(py - r)) + int((idx / side) % side);
+    z = int(floorf(pz - r)) + int(idx % side);
     const bool inside = x >= 0 && x < nx && y >= 0 && y < ny && z >= 0 && z < nz;
     const long long c = ((long long)x * ny + y) * nz + z;
     const bool fluid = inside && (a.w.flag == nullptr || a.w.flag[c] == ML_FLUID) &&
                        (a.w.flag != nullptr || a.w.periodic || (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1));
-    if (fluid && first_near<R>(s, R(x), R(y), R(z)) == k0) {
-      any = true;
-      const Mom3<R> mc = load_cell<S>(a, N, c);
-      R rho_acc = 0, uxp = 0, uxm = 0, uyp = 0, uym = 0, uzp = 0, uzm = 0, pixx = 0, piyy = 0, pizz = 0;
-      R pixy_p = 0, pixy_m = 0, pixz_p = 0, pixz_m = 0, piyz_p = 0, piyz_m = 0;
-      for (int i = 0; i < 27; ++i) {
-        const int ix = c_cx[i], iy = c_cy[i], iz = c_cz[i];
-        const R dx = R(ix), dy = R(iy), dz = R(iz);
-        const R wi = weight<R>(i);
-        int xn = x - ix, yn = y - iy, zn = z - iz;
-        if (a.w.periodic) {
-          xn = wrap(xn, nx);
-          yn = wrap(yn, ny);
-          zn = wrap(zn, nz);
-        }
-        R pop = R(0);
-        if (xn >= 0 && xn < nx && yn >= 0 && yn < ny && zn >= 0 && zn < nz) {
-          // get_cutcell_multi_3d: the closest hit in [0, 1] over the solids near the cell
-          R cut = R(-1);
-          int sid = -1;
-          const V3<R> cell{R(x), R(y), R(z)};
-          const V3<R> dir{-dx, -dy, -dz};
-          for (int k = 0; k < n; ++k) {
-            const int t0 = s.tri_offset[k], ntri = s.tri_offset[k + 1] - t0;
-            if (ntri == 0) continue;
-            if (vlen(cell.x - R(s.position[3 * k]), cell.y - R(s.position[3 * k + 1]), cell.z - R(s.position[3 * k + 2])) >
-                R(s.bound_radius[k]) + R(2))
-              continue;
-            const Xf<R> inv = xinv(load_xf<R>(s.transforms + 7 * k));
-            const V3<R> lo = xpoint(inv, cell);
-            const V3<R> ld = qrot(inv.qx, inv.qy, inv.qz, inv.qw, dir);
-            const R sx = R(s.scale_sizes[3 * k]), sy = R(s.scale_sizes[3 * k + 1]), sz = R(s.scale_sizes[3 * k + 2]);
-            R t;
-            if (ray_mesh<R>(s.tris + 9ll * t0, ntri, {lo.x / sx, lo.y / sy, lo.z / sz}, {ld.x / sx, ld.y / sy, ld.z / sz},
-                            R(2), &t)) {
-              if ((cut < R(0) || t < cut) && t >= R(0) && t <= R(1)) {
-                cut = t;
-                sid = k;
-              }
-            }
-          }
-          if (sid >= 0) {
-            const Xf<R> tc = load_xf<R>(s.transforms + 7 * sid);
-            const Xf<R> tl = load_xf<R>(s.transforms_last + 7 * sid);
-            const V3<R> hit{cell.x + dir.x * cut, cell.y + dir.y * cut, cell.z + dir.z * cut};
-            const V3<R> hl = xpoint(xinv(tc), hit);
-            V3<R> up;
-            const R spx = R(s.position[3 * sid]), spy = R(s.position[3 * sid + 1]), spz = R(s.position[3 * sid + 2]);
-            if (s.initialized[sid] > 0) {
-              const V3<R> pc = xpoint(tc, hl), pl = xpoint(tl, hl);
-              up = {pc.x - pl.x, pc.y - pl.y, pc.z - pl.z};
-            } else {
-              const R ax = R(s.angle_v[3 * sid]), ay = R(s.angle_v[3 * sid + 1]), az = R(s.angle_v[3 * sid + 2]);
-              const R rx = hit.x - spx, ry = hit.y - spy, rz = hit.z - spz;
-              up = {R(s.linear_v[3 * sid]) + (ay * rz - az * ry), R(s.linear_v[3 * sid + 1]) + (az * rx - ax * rz),
-                    R(s.linear_v[3 * sid + 2]) + (ax * ry - ay * rx)};
-            }
-            const R rx = hit.x - spx, ry = hit.y - spy, rz = hit.z - spz;
-            const R Sxx_s = up.x * up.x + mc.sxx - mc.ux * mc.ux;
-            const R Sxy_s = up.x * up.y + mc.sxy - mc.ux * mc.uy;
-            const R Sxz_s = up.x * up.z + mc.sxz - mc.ux * mc.uz;
-            const R Syy_s = up.y * up.y + mc.syy - mc.uy * mc.uy;
-            const R Syz_s = up.y * up.z + mc.syz - mc.uy * mc.uz;
-            const R Szz_s = up.z * up.z + mc.szz - mc.uz * mc.uz;
-            pop = feq<R>(mc.rho, up.x, up.y, up.z, Sxx_s, Sxy_s, Sxz_s, Syy_s, Syz_s, Szz_s, dx, dy, dz, wi);
-            const int ii = inverse(i);
-            const R ex = R(c_cx[ii]), ey = R(c_cy[ii]), ez = R(c_cz[ii]);
-            const R cur_f = feq<R>(mc.rho, mc.ux, mc.uy, mc.uz, mc.sxx, mc.sxy, mc.sxz, mc.syy, mc.syz, mc.szz, ex, ey,
-                                   ez, weight<R>(ii));
-            const R fx = cur_f * (ex - up.x) - pop * (dx - up.x);
-            const R fy = cur_f * (ey - up.y) - pop * (dy - up.y);
-            const R fz = cur_f * (ez - up.z) - pop * (dz - up.z);
-            double* L = acc + 6 * sid;
-            atomicAdd(&L[0], double(fx));
-            atomicAdd(&L[1], double(fy));
-            atomicAdd(&L[2], double(fz));
-            atomicAdd(&L[3], double(ry * fz - rz * fy));
-            atomicAdd(&L[4], double(rz * fx - rx * fz));
-            atomicAdd(&L[5], double(rx * fy - ry * fx));
-          } else {
-            const Mom3<R> m = load_cell<S>(a, N, ((long long)xn * ny + yn) * nz + zn);
-            pop = feq<R>(m.rho, m.ux, m.uy, m.uz, m.sxx, m.sxy, m.sxz, m.syy, m.syz, m.szz, dx, dy, dz, wi);
-            if (pop < R(0)) pop = R(0);
-          }
-        }
-        // moments in the reference's order (528-562)
-        rho_acc = rho_acc + pop;
-        if (ix > 0) { uxp = uxp + pop; pixx = pixx + pop; }
-        else if (ix < 0) { uxm = uxm + pop; pixx = pixx + pop; }
-        if (iy > 0) { uyp = uyp + pop; piyy = piyy + pop; }
-        else if (iy < 0) { uym = uym + pop; piyy = piyy + pop; }
-        if (iz > 0) { uzp = uzp + pop; pizz = pizz + pop; }
-        else if (iz < 0) { uzm = uzm + pop; pizz = pizz + pop; }
-        const int dxy = ix * iy, dxz = ix * iz, dyz = iy * iz;
-        if (dxy > 0) pixy_p = pixy_p + pop;
-        else if (dxy < 0) pixy_m = pixy_m + pop;
-        if (dxz > 0) pixz_p = pixz_p + pop;
-        else if (dxz < 0) pixz_m = pixz_m + pop;
-        if (dyz > 0) piyz_p = piyz_p + pop;
-        else if (dyz < 0) piyz_m = piyz_m + pop;
-      }
-      // regularised collision (564-604)
-      const R Fx = a.w.force ? R(a.w.force[c]) : R(0);
-      const R Fy = a.w.force ? R(a.w.force[N + c]) : R(0);
-      const R Fz = a.w.force ? R(a.w.force[2 * N + c]) : R(0);
-      const R rho = rho_acc;
-      const R invRho = R(1) / rho;
-      const R ux = (uxp - uxm + R(0.5) * Fx) * invRho;
-      const R uy = (uyp - uym + R(0.5) * Fy) * invRho;
-      const R uz = (uzp - uzm + R(0.5) * Fz) * invRho;
-      R pixy = pixy_p - pixy_m, pixz = pixz_p - pixz_m, piyz = piyz_p - piyz_m;
-      const R omega = R(1) / (R(a.vis_shear) * R(3) + R(0.5));
-      const R pixx_part = (R(2) * pixx - piyy - pizz) / R(3);
-      const R piyy_part = (R(2) * piyy - pixx - pizz) / R(3);
-      const R pizz_part = (R(2) * pizz - pixx - piyy) / R(3);
-      const R RU2 = rho * ux * ux, RV2 = rho * uy * uy, RW2 = rho * uz * uz;
-      const R RUVW2 = (RU2 + RV2 + RW2) / R(3);
-      const R o1 = R(1) - omega;
-      const R qxx = rho / R(3) + pixx_part * o1 + RUVW2 + (R(2) * RU2 * omega) / R(3) - (RV2 * omega) / R(3) -
-                    (RW2 * omega) / R(3) + Fx * ux;
-      const R qyy = rho / R(3) + piyy_part * o1 + RUVW2 - (RU2 * omega) / R(3) + (R(2) * RV2 * omega) / R(3) -
-                    (RW2 * omega) / R(3) + Fy * uy;
-      const R qzz = rho / R(3) + pizz_part * o1 + RUVW2 - (RU2 * omega) / R(3) - (RV2 * omega) / R(3) +
-                    (R(2) * RW2 * omega) / R(3) + Fz * uz;
-      pixy = pixy - pixy * omega + ux * uy * rho * omega + (Fy * ux + Fx * uy) / R(2);
-      pixz = pixz - pixz * omega + ux * uz * rho * omega + (Fz * ux + Fx * uz) / R(2);
-      piyz = piyz - piyz * omega + uy * uz * rho * omega + (Fz * uy + Fy * uz) / R(2);
-      const R cs2 = R(1.0 / 3.0);
-      Mom3<R> m;
-      m.rho = rho;
-      m.drho = rho - R(1);
-      m.ux = ux + Fx * invRho / R(2);
-      m.uy = uy + Fy * invRho / R(2);
-      m.uz = uz + Fz * invRho / R(2);
-      m.sxx = qxx * invRho - cs2;
-      m.syy = qyy * invRho - cs2;
-      m.szz = qzz * invRho - cs2;
-      m.sxy = pixy * invRho;
-      m.sxz = pixz * invRho;
-      m.syz = piyz * invRho;
-      R raw[10];
-      encode3<S>(m, a.sc, raw);
-      T* post = static_cast<T*>(a.w.post);
-#pragma unroll
-      for (int k = 0; k < 10; ++k) post[k * N + c] = S::from_r(raw[k]);
-    }
+    flagged = fluid && first_near<R>(s, R(x), R(y), R(z)) == k0 && may_cut<R>(s, V3<R>{R(x), R(y), R(z)});
+  }
+  // 2. the warp computes its flagged cells one after another, a lane per direction
+  unsigned mask = __ballot_sync(0xffffffffu, flagged);
+  const bool any = mask != 0;
+  while (mask) {
+    const int src = __ffs(mask) - 1;
+    mask &= mask - 1;
+    const int cx = __shfl_sync(0xffffffffu, x, src), cy = __shfl_sync(0xffffffffu, y, src),
+              cz = __shfl_sync(0xffffffffu, z, src);
+    cut_cell<S>(a, acc, cx, cy, cz);
+    __syncwarp();
+  }
+  if (!__syncthreads_or(any)) return;
+  for (int k = threadIdx.x; k < 6 * n; k += blockDim.x)
+    if (acc[k] != 0.0) atomicAdd(&s.loads64[k], acc[k]);
+}
+
+// Work-list form. classify_kernel: one thread per box cell appends the cells that can have a
+// cut link to work[1..] (count in work[0], one atomic per warp); process_kernel: a fixed grid
+// of warps takes the listed cells in turn, a cell per warp as in band_kernel.
+template <class S> __global__ void __launch_bounds__(BLOCK) classify_kernel(const __grid_constant__ Args a) {
+  using R = typename S::R;
+  const hl_solids3d& s = a.s;
+  const int k0 = blockIdx.y;
+  const int nx = a.w.nx, ny = a.w.ny, nz = a.w.nz;
+  const float px = s.position[3 * k0], py = s.position[3 * k0 + 1], pz = s.position[3 * k0 + 2];
+  const float r = s.bound_radius[k0] + 2.f;
+  const int side = a.box_side;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool flagged = false;
+  int c = 0;
+  if (s.tri_offset[k0 + 1] > s.tri_offset[k0] && isfinite(px) && isfinite(py) && isfinite(pz) && isfinite(r) &&
+      idx < (long long)side * side * side) {
+    const int x = int(floorf(px - r)) + int(idx / ((long long)side * side));
+    const int y = int(floorf(py - r)) + int((idx / side) % side);
+    const int z = int(floorf(pz - r)) + int(idx % side);
+    const bool inside = x >= 0 && x < nx && y >= 0 && y < ny && z >= 0 && z < nz;
+    c = (x * ny + y) * nz + z;
+    const bool fluid = inside && (a.w.flag == nullptr || a.w.flag[c] == ML_FLUID) &&
+                       (a.w.flag != nullptr || a.w.periodic || (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1));
+    flagged = fluid && first_near<R>(s, R(x), R(y), R(z)) == k0 && may_cut<R>(s, V3<R>{R(x), R(y), R(z)});
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, flagged);
+  if (mask == 0) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(s.work, __popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (flagged) s.work[1 + base + __popc(mask & ((1u << lane) - 1))] = c;
+}
+
+template <class S> __global__ void __launch_bounds__(BLOCK) process_kernel(const __grid_constant__ Args a) {
+  __shared__ double acc[MAX_SOLIDS * 6];
+  const hl_solids3d& s = a.s;
+  const int n = s.n_objects;
+  for (int k = threadIdx.x; k < 6 * n; k += blockDim.x) acc[k] = 0.0;
+  __syncthreads();
+  const int count = s.work[0];
+  const int warps = gridDim.x * (BLOCK / 32);
+  const int ny = a.w.ny, nz = a.w.nz;
+  bool any = false;
+  for (int j = blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5); j < count; j += warps) {
+    const int c = s.work[1 + j];
+    any = true;
+    cut_cell<S>(a, acc, c / (ny * nz), (c / nz) % ny, c % nz);
+    __syncwarp();
   }
   if (!__syncthreads_or(any)) return;
   for (int k = threadIdx.x; k < 6 * n; k += blockDim.x)
@@ -334,6 +469,19 @@ __global__ void loads_out_kernel(hl_solids3d s) {
   }
 }
 
+int num_sms_local() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+int box_side_of(float max_bound_radius) { return int(ceilf(2.f * (max_bound_radius + 2.f))) + 2; }
+
 template <class S> int launch(const hl_world3d* w, double vis, const hl_solids3d* s, cudaStream_t st) {
   Args a;
   a.w = *w;
@@ -341,11 +489,20 @@ template <class S> int launch(const hl_world3d* w, double vis, const hl_solids3d
   a.s = *s;
   a.sc = make_scale(w->storage);
   // cells within r = max_bound_radius + 2 of a point lie in floor(p - r) .. floor(p - r) + side - 1
-  a.box_side = int(ceilf(2.f * (s->max_bound_radius + 2.f))) + 2;
+  a.box_side = box_side_of(s->max_bound_radius);
   const long long cells = (long long)a.box_side * a.box_side * a.box_side;
   const dim3 grid(unsigned((cells + BLOCK - 1) / BLOCK), unsigned(s->n_objects));
-  band_kernel<S><<<grid, BLOCK, 0, st>>>(a);
-  HL_LAUNCH_CHECK("d3q27 solid links (band)");
+  if (s->work != nullptr) {
+    cudaError_t e = cudaMemsetAsync(s->work, 0, sizeof(int32_t), st);
+    if (e != cudaSuccess) return cuda_status(e, "d3q27 solid links: zero work count");
+    classify_kernel<S><<<grid, BLOCK, 0, st>>>(a);
+    HL_LAUNCH_CHECK("d3q27 solid links (classify)");
+    process_kernel<S><<<unsigned(4 * num_sms_local()), BLOCK, 0, st>>>(a);
+    HL_LAUNCH_CHECK("d3q27 solid links (cut cells)");
+  } else {
+    band_kernel<S><<<grid, BLOCK, 0, st>>>(a);
+    HL_LAUNCH_CHECK("d3q27 solid links (band)");
+  }
   loads_out_kernel<<<(s->n_objects + 63) / 64, 64, 0, st>>>(*s);
   HL_LAUNCH_CHECK("d3q27 solid links (loads)");
   return HL_OK;
@@ -380,4 +537,10 @@ extern "C" int hl_d3q27_solid_links(const hl_world3d* w, double vis_shear, const
   }
   set_error("d3q27 solid links: storage dtype %d not supported", int(w->storage.dtype));
   return HL_ERR_UNSUPPORTED;
+}
+
+extern "C" size_t hl_d3q27_solid_links_work_ints(int n_objects, float max_bound_radius) {
+  if (n_objects <= 0 || !(max_bound_radius >= 0.f) || max_bound_radius >= 512.f) return 0;
+  const size_t side = size_t(d3s::box_side_of(max_bound_radius));
+  return 1 + size_t(n_objects) * side * side * side;
 }

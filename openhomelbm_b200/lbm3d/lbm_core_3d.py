@@ -35,12 +35,15 @@ class HomeFlow3D:
 
     def Initialize(self, nx: int, ny: int, nz: int, n_objects: int = 1, *, device=None,
                    storage: str = "float32", u_scale: float = 1.0, s_scale: float = 1.0,
-                   periodic: bool = False) -> None:
+                   periodic: bool = False, with_flag: bool = True, with_force: bool = True) -> None:
         """Allocate the fields (reference: HomeFlow3D.Initialize, lbm_core_3d.py:138-227).
 
         ``storage`` selects the moment storage type ("float32", "float16", "bfloat16",
         "float64"); reduced types store rho-1, u/u_scale and (S-uu)/s_scale. ``periodic``
         makes every cell fluid with periodic neighbours (no walls, no apply_bc_3d).
+        ``with_flag=False`` skips the flag field (the border cells are the walls, as
+        InitBoundary3D would set them) and ``with_force=False`` the body-force field: a
+        resident domain that needs neither then holds only its two moment buffers.
         """
         dev = _lib.require_cuda(device)
         self.device = dev
@@ -60,8 +63,9 @@ class HomeFlow3D:
         shape = (10, self.nx, self.ny, self.nz)
         self.moments = [torch.zeros(shape, dtype=tdt, device=dev), torch.zeros(shape, dtype=tdt, device=dev)]
         self.parity = 0
-        self.flag = torch.zeros((self.nx, self.ny, self.nz), dtype=torch.int32, device=dev)
-        self.force = torch.zeros((3, self.nx, self.ny, self.nz), dtype=torch.float32, device=dev)
+        self.flag = torch.zeros((self.nx, self.ny, self.nz), dtype=torch.int32, device=dev) if with_flag else None
+        self.force = (torch.zeros((3, self.nx, self.ny, self.nz), dtype=torch.float32, device=dev) if with_force
+                      else None)
         self.use_force = False
         n = self.n_objects
         f32 = dict(dtype=torch.float32, device=dev)
@@ -142,9 +146,9 @@ class HomeFlow3D:
     Sxy_post = property(lambda s: s._plane(7, True))
     Sxz_post = property(lambda s: s._plane(8, True))
     Syz_post = property(lambda s: s._plane(9, True))
-    forcex = property(lambda s: s.force[0])
-    forcey = property(lambda s: s.force[1])
-    forcez = property(lambda s: s.force[2])
+    forcex = property(lambda s: None if s.force is None else s.force[0])
+    forcey = property(lambda s: None if s.force is None else s.force[1])
+    forcez = property(lambda s: None if s.force is None else s.force[2])
 
     # ------------------------------------------------------------------ ABI structs
     def world_struct(self, parity: Optional[int] = None) -> _lib.hl_world3d:
@@ -154,8 +158,8 @@ class HomeFlow3D:
         w.storage = _lib.hl_storage(self.storage_code, self.u_scale, self.s_scale)
         w.cur = self.moments[p].data_ptr()
         w.post = self.moments[p ^ 1].data_ptr()
-        w.flag = None if self.periodic else self.flag.data_ptr()
-        w.force = self.force.data_ptr() if self.use_force else None
+        w.flag = None if (self.periodic or self.flag is None) else self.flag.data_ptr()
+        w.force = self.force.data_ptr() if (self.use_force and self.force is not None) else None
         w.periodic = int(self.periodic)
         return w
 

@@ -19,12 +19,58 @@ from .. import _lib
 from .lbm_core_3d import HomeFlow3D
 
 
+_BIN_CACHE: Dict[Tuple, Tuple] = {}
+
+
+def triangle_bins(tris: np.ndarray, margin: float = 1.75, edge: float = 1.0, max_bins: int = 1 << 20):
+    """Uniform grid of triangle lists over a body-frame mesh (T, 3, 3), for the link rays of
+    the cut cells. Bin b lists every triangle whose bounding box, widened by ``margin`` (more
+    than sqrt(3), the longest lattice link), meets b; the grid spans the mesh's bounding box
+    widened the same way, so a ray of length <= sqrt(3) starting outside the grid hits nothing.
+    Returns (origin x, y, z, edge), (nbx, nby, nbz), CSR starts (nbins + 1) and the lists.
+    An empty mesh gives a 0 x 0 x 0 grid. Results are cached by mesh content."""
+    if len(tris) == 0:
+        return [0.0, 0.0, 0.0, 1.0], (0, 0, 0), np.zeros(1, np.int64), np.zeros(0, np.int64)
+    t = np.ascontiguousarray(tris, np.float32)
+    key = (t.shape, t.tobytes(), margin, edge, max_bins)
+    hit = _BIN_CACHE.get(key)
+    if hit is not None:
+        return hit
+    t = t.astype(np.float64)
+    lo = t.min(axis=(0, 1)) - margin
+    hi = t.max(axis=(0, 1)) + margin
+    dims = np.maximum(np.ceil((hi - lo) / edge), 1).astype(np.int64)
+    if dims.prod() > max_bins:
+        edge *= (dims.prod() / max_bins) ** (1.0 / 3.0) * 1.001
+        dims = np.maximum(np.ceil((hi - lo) / edge), 1).astype(np.int64)
+    i0 = np.clip(np.floor((t.min(axis=1) - margin - lo) / edge).astype(np.int64), 0, dims - 1)
+    i1 = np.clip(np.floor((t.max(axis=1) + margin - lo) / edge).astype(np.int64), 0, dims - 1)
+    span = i1 - i0 + 1                       # (T, 3) bins per axis
+    count = span.prod(axis=1)                # bins per triangle
+    tri_ids = np.repeat(np.arange(len(t)), count)
+    local = np.arange(count.sum()) - np.repeat(np.cumsum(count) - count, count)
+    sy, sz = np.repeat(span[:, 1], count), np.repeat(span[:, 2], count)
+    gx = np.repeat(i0[:, 0], count) + local // (sy * sz)
+    gy = np.repeat(i0[:, 1], count) + (local // sz) % sy
+    gz = np.repeat(i0[:, 2], count) + local % sz
+    bins = (gx * dims[1] + gy) * dims[2] + gz
+    order = np.lexsort((tri_ids, bins))
+    bins, tri_ids = bins[order], tri_ids[order]
+    start = np.searchsorted(bins, np.arange(dims.prod() + 1))
+    out = ([float(lo[0]), float(lo[1]), float(lo[2]), float(edge)], tuple(int(d) for d in dims), start, tri_ids)
+    if len(_BIN_CACHE) > 64:
+        _BIN_CACHE.clear()
+    _BIN_CACHE[key] = out
+    return out
+
+
 class LBM_Solver3D:
     """Advance one or more D3Q27 fluid worlds on a CUDA device."""
 
     def __init__(self, nx: int, ny: int, nz: int, solid_num: int = 1, nworld: int = 1,
                  device: Optional[Any] = None, *, storage: str = "float32", periodic: bool = False,
-                 u_scale: float = 1.0, s_scale: float = 1.0, use_graph: bool = True) -> None:
+                 u_scale: float = 1.0, s_scale: float = 1.0, use_graph: bool = True, with_flag: bool = True,
+                 with_force: bool = True) -> None:
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.solid_num = int(solid_num)
         self.nworld = int(nworld)
@@ -38,12 +84,13 @@ class LBM_Solver3D:
         for _ in range(self.nworld):
             f = HomeFlow3D()
             f.Initialize(nx, ny, nz, n_objects=solid_num, device=self.device, storage=storage,
-                         u_scale=u_scale, s_scale=s_scale, periodic=periodic)
+                         u_scale=u_scale, s_scale=s_scale, periodic=periodic, with_flag=with_flag,
+                         with_force=with_force)
             self.flows.append(f)
         stream = _lib.stream_ptr()
         L = _lib.lib()
         for f in self.flows:
-            if not periodic:
+            if not periodic and f.flag is not None:
                 _lib.check(L.hl_d3q27_init_boundary(f.nx, f.ny, f.nz, _lib.ptr(f.flag), stream),
                            "InitBoundary3D")
             _lib.check(L.hl_d3q27_init_uniform(f.nx, f.ny, f.nz, _lib.hl_storage(f.storage_code, f.u_scale, f.s_scale),
@@ -63,6 +110,8 @@ class LBM_Solver3D:
         self._tri_offset = torch.zeros(self.solid_num + 1, dtype=torch.int32, device=self.device)
         self._max_bound_radius = 0.0
         self._solid_version = 0
+        self.use_bins = True
+        self.use_work_list = True
         self._batch_solid_state()
         self.mujoco_mappings = {}
         self.mujoco_origins_wp = None
@@ -121,6 +170,13 @@ class LBM_Solver3D:
         s.loads64 = f.loads64.data_ptr()
         s.force = f.solid_force.data_ptr()
         s.torque = f.solid_torque.data_ptr()
+        if self.use_bins:
+            s.bin_box = self._bin_box.data_ptr()
+            s.bin_dims = self._bin_dims.data_ptr()
+            s.bin_start = self._bin_start.data_ptr()
+            s.bin_tris = self._bin_tris.data_ptr()
+        if self.use_work_list:
+            s.work = self._link_work[k].data_ptr()
         return s
 
     @property
@@ -272,8 +328,25 @@ class LBM_Solver3D:
         allt = np.concatenate(tris) if sum(counts) else np.zeros((1, 3, 3), np.float32)
         self._tris = torch.tensor(np.ascontiguousarray(allt, np.float32), device=self.device)
         self._tri_offset = torch.tensor(offs, device=self.device)
+        boxes, dims, starts, lists = [], [], [], []
+        first_bin = first_tri = 0
+        for t in tris:
+            box, d, start, lst = triangle_bins(t)
+            boxes.append(box)
+            dims.append([d[0], d[1], d[2], first_bin])
+            starts.append(start + first_tri)
+            lists.append(lst)
+            first_bin += len(start)
+            first_tri += len(lst)
+        dev = self.device
+        self._bin_box = torch.tensor(np.array(boxes, np.float32), device=dev)
+        self._bin_dims = torch.tensor(np.array(dims, np.int32), device=dev)
+        self._bin_start = torch.tensor(np.concatenate(starts).astype(np.int32), device=dev)
+        self._bin_tris = torch.tensor(np.concatenate(lists + [np.zeros(1, np.int32)]).astype(np.int32), device=dev)
         radii = [float(np.linalg.norm(t.reshape(-1, 3), axis=1).max()) for t in tris if len(t)]
         self._max_bound_radius = max(radii) if radii else 0.0
+        ints = int(_lib.lib().hl_d3q27_solid_links_work_ints(self.solid_num, float(self._max_bound_radius)))
+        self._link_work = [torch.zeros(max(ints, 1), dtype=torch.int32, device=dev) for _ in self.flows]
         self._solid_version += 1
 
     def _update_mesh_transform(self, flow: HomeFlow3D, solid_id: int) -> None:

@@ -1,0 +1,393 @@
+"""Serving form: a request loop of mesh-coupled D3Q27 domains kept resident on the GPU.
+
+Each request is one RL environment's flow: a cubic domain with a 5-segment swimmer whose yaw
+joints follow seeded sinusoids; the caller wants per-segment force and torque after every
+control step (``substeps`` LBM steps), for ``control_steps`` control steps.
+
+``ServeEngine`` runs requests with continuous batching: a request that has arrived is admitted
+as soon as a slot is free and its fields fit the HBM budget; its fields stay on the device for
+its whole life; every active request advances one control step per tick, each on its own CUDA
+stream, so the domains' kernels overlap on the device (the small domains fill the SMs the big
+ones leave idle). A domain's control step (pose updates, stream-collide, cut links, boundaries
+and load copies for all substeps) is captured once into a CUDA graph at admission, so a tick
+is one graph launch per domain, and the poses of every domain's next control step are computed
+on the host while the tick runs on the device. Admission (allocation, initial state, graph
+capture) happens between ticks and counts in the wall time, not in a control step's latency.
+``run_plain`` is the baseline: the same requests one at a time through the plain drop-in
+solver (LBM_Solver3D, float32 storage), one graph launch per LBM step.
+
+Every domain's result is independent of the others in the mix: the kernels of one domain
+read and write only that domain's buffers.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+from .lbm3d import LBM_Solver3D
+
+SEGMENTS = 5
+
+
+# ----------------------------------------------------------------------------- bodies
+def ellipsoid_mesh(a: float, b: float, c: float, n_lon: int = 20, n_lat: int = 11) -> Tuple[np.ndarray, np.ndarray]:
+    """Closed triangle mesh of an ellipsoid with semi-axes (a, b, c) centred at (a, 0, 0), so
+    that its joint (the body-frame origin) sits on its back end: 2 n_lon (n_lat - 2) triangles
+    (360 for the defaults)."""
+    verts = [(0.0, 0.0, 0.0)]  # back pole (x = 0)
+    for i in range(1, n_lat - 1):
+        th = math.pi * i / (n_lat - 1)
+        for j in range(n_lon):
+            ph = 2 * math.pi * j / n_lon
+            verts.append((a - a * math.cos(th), b * math.sin(th) * math.cos(ph), c * math.sin(th) * math.sin(ph)))
+    verts.append((2 * a, 0.0, 0.0))  # front pole
+    faces = []
+    ring = lambda i, j: 1 + (i - 1) * n_lon + (j % n_lon)
+    for j in range(n_lon):
+        faces.append((0, ring(1, j + 1), ring(1, j)))
+    for i in range(1, n_lat - 2):
+        for j in range(n_lon):
+            faces.append((ring(i, j), ring(i, j + 1), ring(i + 1, j)))
+            faces.append((ring(i, j + 1), ring(i + 1, j + 1), ring(i + 1, j)))
+    last = len(verts) - 1
+    for j in range(n_lon):
+        faces.append((last, ring(n_lat - 2, j), ring(n_lat - 2, j + 1)))
+    return np.array(verts, np.float64), np.array(faces, np.int64)
+
+
+@dataclass
+class Swimmer:
+    """A chain of SEGMENTS ellipsoids joined by yaw joints. Segment k's body frame has its
+    joint at the origin; joint angle k follows amp[k] sin(2 pi freq t + phase[k]) (t in LBM
+    steps), and the head's joint is fixed at ``head``. The amplitudes grow towards the tail and
+    the frequency is set from a seeded peak wall speed of 0.02-0.04 lattice units per step
+    (the bound omega L sum_k amp[k] (SEGMENTS - k) of the tail's speed), well inside the
+    low-Mach range of the lattice whatever the domain size."""
+
+    side: int
+    seg_len: float
+    head: np.ndarray
+    amp: np.ndarray
+    freq: float
+    phase: np.ndarray
+    meshes: List[Tuple[np.ndarray, np.ndarray]] = field(default_factory=list)
+
+    @staticmethod
+    def make(side: int, rng: np.random.Generator) -> "Swimmer":
+        L = 0.1 * side
+        meshes = [ellipsoid_mesh(L / 2, 0.18 * L, 0.14 * L) for _ in range(SEGMENTS)]
+        head = np.array([0.3 * side, 0.5 * side + rng.uniform(-1, 1), 0.5 * side + rng.uniform(-1, 1)])
+        amp = 0.15 * rng.uniform(0.8, 1.2) * (0.2 + 0.2 * np.arange(SEGMENTS))
+        v_peak = rng.uniform(0.02, 0.04)
+        freq = v_peak / (2 * np.pi * L * float(np.sum(amp * (SEGMENTS - np.arange(SEGMENTS)))))
+        return Swimmer(side, L, head, amp, float(freq), rng.uniform(0, 2 * np.pi, SEGMENTS), meshes)
+
+    def poses(self, t: float) -> Tuple[np.ndarray, np.ndarray]:
+        """Joint positions (SEGMENTS, 3) and orientations (SEGMENTS, 4) as (w, x, y, z)."""
+        pos = np.zeros((SEGMENTS, 3))
+        quat = np.zeros((SEGMENTS, 4))
+        p = self.head.astype(np.float64).copy()
+        yaw = 0.0
+        for k in range(SEGMENTS):
+            yaw += self.amp[k] * math.sin(2 * math.pi * self.freq * t + self.phase[k])
+            pos[k] = p
+            quat[k] = (math.cos(yaw / 2), 0.0, 0.0, math.sin(yaw / 2))
+            p = p + self.seg_len * np.array([math.cos(yaw), math.sin(yaw), 0.0])
+        return pos.astype(np.float32), quat.astype(np.float32)
+
+
+@dataclass
+class Request:
+    """One environment: domain side, body seed, arrival time (s after the loop starts)."""
+
+    rid: int
+    side: int
+    seed: int
+    arrival: float = 0.0
+    control_steps: int = 100
+    substeps: int = 8
+
+
+def poisson_requests(n: int, rate: float, seed: int, side_lo: int = 64, side_hi: int = 192, round_to: int = 32,
+                     control_steps: int = 100, substeps: int = 8) -> List[Request]:
+    """n requests with exponential inter-arrival times (rate per second) and cubic sides drawn
+    log-uniform in [side_lo, side_hi], rounded to a multiple of ``round_to`` (the TMA kernel's
+    tile: 16 in y, 32 in z)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n)) if rate > 0 else np.zeros(n)
+    sides = np.exp(rng.uniform(math.log(side_lo), math.log(side_hi), n))
+    sides = np.clip(np.round(sides / round_to) * round_to, side_lo, side_hi).astype(int)
+    return [Request(i, int(sides[i]), int(rng.integers(1 << 30)), float(t[i]), control_steps, substeps)
+            for i in range(n)]
+
+
+def domain_bytes(side: int, storage: str) -> int:
+    """Device bytes a resident domain holds: two moment buffers plus the per-solid state."""
+    bpc = {"float32": 40, "float16": 20, "bfloat16": 20, "float64": 80}[storage]
+    return 2 * side ** 3 * bpc + (1 << 20)
+
+
+# ----------------------------------------------------------------------------- one domain
+class Domain:
+    """A resident request: its solver (one world), swimmer, pose and load buffers, stream and
+    the CUDA graph of one control step."""
+
+    def __init__(self, req: Request, storage: str, vis: float, device, use_graph: bool = True):
+        self.req = req
+        self.device = device
+        self.stream = torch.cuda.Stream(device=device)
+        self.done = 0
+        self.latencies: List[float] = []
+        self.loads: List[np.ndarray] = []
+        n = req.side
+        with torch.cuda.stream(self.stream):
+            self.solver = LBM_Solver3D(n, n, n, solid_num=SEGMENTS, storage=storage, device=device, use_graph=False,
+                                       u_scale=0.02, s_scale=4e-4, with_flag=False, with_force=False)
+            self.solver.set_viscosity(vis)
+            self.swimmer = Swimmer.make(n, np.random.default_rng(req.seed))
+            pos, quat = self.swimmer.poses(0.0)
+            for k, mesh in enumerate(self.swimmer.meshes):
+                self.solver.create_solid_from_mesh(k, mesh, lbm_position=tuple(pos[k]), lbm_scale=1.0 / n,
+                                                   init_quaternion=tuple(quat[k]))
+            S, dev = req.substeps, device
+            # poses of every substep of a control step: positions and quaternions (w, x, y, z);
+            # two pinned host copies so the next step's poses are written while the device
+            # still reads the current ones
+            self.pos_host = [torch.zeros((S, SEGMENTS, 3), dtype=torch.float32).pin_memory() for _ in range(2)]
+            self.quat_host = [torch.zeros((S, SEGMENTS, 4), dtype=torch.float32).pin_memory() for _ in range(2)]
+            self.pos_dev = torch.zeros((S, SEGMENTS, 3), dtype=torch.float32, device=dev)
+            self.quat_dev = torch.zeros((S, SEGMENTS, 4), dtype=torch.float32, device=dev)
+            self.buf = 0
+            self.loads_dev = torch.zeros((S, SEGMENTS, 6), dtype=torch.float32, device=dev)
+            self.loads_host = torch.zeros((S, SEGMENTS, 6), dtype=torch.float32).pin_memory()
+            self.ids = torch.arange(SEGMENTS, dtype=torch.int32, device=dev)
+            self.zeros3 = torch.zeros((SEGMENTS, 3), dtype=torch.float32, device=dev)
+            self.ones = torch.ones(SEGMENTS, dtype=torch.float32, device=dev)
+        self.graph = None
+        if use_graph:
+            self.stream.synchronize()
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph, stream=self.stream):
+                self._control_step()
+        self.event = torch.cuda.Event()
+
+    def _control_step(self) -> None:
+        """One control step on the current stream: per substep, the swimmer's pose from the
+        pose buffer (convert_and_update_solid_batch_3d), one LBM step with the cut links, and
+        a copy of the segments' loads."""
+        s = self.solver
+        L = _lib.lib()
+        st = _lib.stream_ptr()
+        f = s.flows[0]
+        for k in range(self.req.substeps):
+            _lib.check(L.hl_couple3d_update_solids(
+                1, SEGMENTS, SEGMENTS, _lib.ptr(self.ids), self.pos_dev[k].data_ptr(), self.quat_dev[k].data_ptr(),
+                _lib.ptr(self.zeros3), _lib.ptr(self.zeros3), _lib.ptr(self.ones),
+                _lib.ptr(s.solid_position_all), _lib.ptr(s.solid_quaternion_all), _lib.ptr(s.mesh_transforms_all),
+                _lib.ptr(s.mesh_transforms_last_all), _lib.ptr(s.mesh_transforms_initialized_all), st),
+                "pose update")
+            s._launch(k % 2, st)
+            self.loads_dev[k, :, :3].copy_(f.solid_force)
+            self.loads_dev[k, :, 3:].copy_(f.solid_torque)
+
+    def stage_poses(self, step: int) -> None:
+        """Host: the swimmer's poses for every substep of control step ``step``, into the host
+        buffer that the launch of that step uploads."""
+        S = self.req.substeps
+        buf = step % 2
+        for k in range(S):
+            pos, quat = self.swimmer.poses(step * S + k + 1)
+            self.pos_host[buf][k] = torch.from_numpy(pos)
+            self.quat_host[buf][k] = torch.from_numpy(quat)
+
+    def launch(self) -> None:
+        """Enqueue the next control step on the domain's stream (pose upload, the step, the
+        load download)."""
+        buf = self.done % 2
+        with torch.cuda.stream(self.stream):
+            self.pos_dev.copy_(self.pos_host[buf], non_blocking=True)
+            self.quat_dev.copy_(self.quat_host[buf], non_blocking=True)
+            if self.graph is not None:
+                self.graph.replay()
+            else:
+                self._control_step()
+            self.loads_host.copy_(self.loads_dev, non_blocking=True)
+            self.event.record(self.stream)
+
+    def finish(self, latency: float) -> None:
+        self.loads.append(self.loads_host.numpy().copy())
+        self.latencies.append(latency)
+        self.done += 1
+
+    @property
+    def finished(self) -> bool:
+        return self.done >= self.req.control_steps
+
+    def release(self) -> None:
+        self.graph = None
+        self.solver = None
+
+
+# ----------------------------------------------------------------------------- engines
+@dataclass
+class ServeStats:
+    env_steps: int
+    wall_s: float
+    latencies_s: List[float]
+    results: Dict[int, np.ndarray]
+    max_active: int
+    admitted_order: List[int]
+
+    @property
+    def env_steps_per_s(self) -> float:
+        return self.env_steps / self.wall_s
+
+    def pct(self, q: float) -> float:
+        return float(np.percentile(np.array(self.latencies_s), q))
+
+
+class ServeEngine:
+    """Continuous batching of resident domains (see the module docstring)."""
+
+    def __init__(self, storage: str = "float16", budget_bytes: float = 150e9, max_active: int = 32,
+                 vis: float = 0.01, device=None):
+        self.storage = storage
+        self.budget = float(budget_bytes)
+        self.max_active = int(max_active)
+        self.vis = float(vis)
+        self.device = _lib.require_cuda(device)
+
+    def run(self, requests: List[Request], realtime: bool = True) -> ServeStats:
+        """Serve the requests (arrival times honoured when ``realtime``) until all finish."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        active: List[Domain] = []
+        used = 0.0
+        lat, results, order = [], {}, []
+        peak = 0
+        steps = 0
+        t_start = time.perf_counter()
+
+        def now():
+            return time.perf_counter() - t_start
+
+        def admit():
+            nonlocal used
+            while pending and len(active) < self.max_active and (not realtime or pending[0].arrival <= now()):
+                need = domain_bytes(pending[0].side, self.storage)
+                if used + need > self.budget:
+                    break
+                r = pending.pop(0)
+                d = Domain(r, self.storage, self.vis, self.device)
+                d.stage_poses(0)
+                active.append(d)
+                used += need
+                order.append(r.rid)
+
+        while pending or active:
+            admit()
+            if not active:
+                time.sleep(max(0.0, min(pending[0].arrival - now(), 0.01)))
+                continue
+            peak = max(peak, len(active))
+            running = list(active)
+            t0 = time.perf_counter()
+            for d in running:
+                d.launch()
+            # while the device works: the poses of every domain's next control step
+            for d in running:
+                if d.done + 1 < d.req.control_steps:
+                    d.stage_poses(d.done + 1)
+            for d in running:
+                d.event.synchronize()
+            t1 = time.perf_counter()
+            for d in running:
+                d.finish(t1 - t0)
+                lat.append(t1 - t0)
+                steps += 1
+            for d in [d for d in active if d.finished]:
+                active.remove(d)
+                results[d.req.rid] = np.stack(d.loads)
+                used -= domain_bytes(d.req.side, self.storage)
+                d.release()
+        torch.cuda.synchronize()
+        return ServeStats(steps, time.perf_counter() - t_start, lat, results, peak, order)
+
+
+def run_plain(requests: List[Request], storage: str = "float32", vis: float = 0.01, device=None) -> ServeStats:
+    """Baseline: one request at a time through the plain solver (LBM_Solver3D.step, one graph
+    launch per LBM step), poses through the coupling kernel, loads read back every control
+    step; requests in arrival order, each started when it has arrived and the previous one
+    finished."""
+    device = _lib.require_cuda(device)
+    lat, results, order = [], {}, []
+    steps = 0
+    t_start = time.perf_counter()
+    for r in sorted(requests, key=lambda r: r.arrival):
+        wait = r.arrival - (time.perf_counter() - t_start)
+        if wait > 0:
+            time.sleep(wait)
+        d = PlainDomain(r, storage, vis, device)
+        for _ in range(r.control_steps):
+            t0 = time.perf_counter()
+            d.control_step()
+            lat.append(time.perf_counter() - t0)
+            steps += 1
+        results[r.rid] = np.stack(d.loads)
+        order.append(r.rid)
+    torch.cuda.synchronize()
+    return ServeStats(steps, time.perf_counter() - t_start, lat, results, 1, order)
+
+
+class PlainDomain:
+    """A request on the plain solver: LBM_Solver3D.step() per substep (its own CUDA graph)."""
+
+    def __init__(self, req: Request, storage: str, vis: float, device):
+        n = req.side
+        self.req = req
+        self.solver = LBM_Solver3D(n, n, n, solid_num=SEGMENTS, storage=storage, device=device, u_scale=0.02,
+                                   s_scale=4e-4, with_flag=False, with_force=False)
+        self.solver.set_viscosity(vis)
+        self.swimmer = Swimmer.make(n, np.random.default_rng(req.seed))
+        pos, quat = self.swimmer.poses(0.0)
+        for k, mesh in enumerate(self.swimmer.meshes):
+            self.solver.create_solid_from_mesh(k, mesh, lbm_position=tuple(pos[k]), lbm_scale=1.0 / n,
+                                               init_quaternion=tuple(quat[k]))
+        self.done = 0
+        self.loads: List[np.ndarray] = []
+        dev = device
+        self.ids = torch.arange(SEGMENTS, dtype=torch.int32, device=dev)
+        self.zeros3 = torch.zeros((SEGMENTS, 3), dtype=torch.float32, device=dev)
+        self.ones = torch.ones(SEGMENTS, dtype=torch.float32, device=dev)
+        S = req.substeps
+        self.pos_host = torch.zeros((S, 1, SEGMENTS, 3), dtype=torch.float32).pin_memory()
+        self.quat_host = torch.zeros((S, 1, SEGMENTS, 4), dtype=torch.float32).pin_memory()
+        self.pos_dev = torch.zeros((S, 1, SEGMENTS, 3), dtype=torch.float32, device=dev)
+        self.quat_dev = torch.zeros((S, 1, SEGMENTS, 4), dtype=torch.float32, device=dev)
+        self.loads_dev = torch.zeros((req.substeps, SEGMENTS, 6), dtype=torch.float32, device=dev)
+
+    def control_step(self) -> None:
+        from . import coupling
+
+        s, S = self.solver, self.req.substeps
+        t0 = self.done * S
+        for k in range(S):
+            pos, quat = self.swimmer.poses(t0 + k + 1)
+            self.pos_host[k, 0] = torch.from_numpy(pos)
+            self.quat_host[k, 0] = torch.from_numpy(quat)
+        self.pos_dev.copy_(self.pos_host, non_blocking=True)
+        self.quat_dev.copy_(self.quat_host, non_blocking=True)
+        f = s.flows[0]
+        for k in range(S):
+            coupling.convert_and_update_solid_batch_3d(s, self.ids, self.pos_dev[k], self.quat_dev[k], self.zeros3,
+                                                       self.zeros3, self.ones)
+            s.step()
+            self.loads_dev[k, :, :3].copy_(f.solid_force)
+            self.loads_dev[k, :, 3:].copy_(f.solid_torque)
+        self.loads.append(self.loads_dev.cpu().numpy())
+        self.done += 1
