@@ -398,6 +398,92 @@ def run_precision(args):
             "results": res}
 
 
+# ----------------------------------------------------------------------------- Karman form
+def shedding_stats(drag, lift, diameter=24.0, u_in=0.05):
+    """Mean drag, lift standard deviation and Strouhal number f D / U from the mean period of
+    the lift's upward zero crossings about its mean (series sampled every step)."""
+    l = lift - lift.mean()
+    up = np.where((l[:-1] < 0) & (l[1:] >= 0))[0]
+    period = float(np.diff(up).mean()) if len(up) > 1 else float("nan")
+    return {"mean_drag": float(drag.mean()), "lift_std": float(lift.std()), "periods": int(len(up) - 1),
+            "period_steps": period, "strouhal": diameter / u_in / period}
+
+
+def run_karman(args):
+    """The D2Q9 Karman configuration: 512 x 128, 96-gon cylinder of radius 12 at (128, 64),
+    inflow (0.05, 0), zero gradient elsewhere, nu = 0.012 (Re 100), rho = 1 and u = inflow plus
+    seeded +-1e-3 noise. 100000 steps on the GPU with drag and lift recorded every step; the
+    shedding statistics over steps 70000-100000 against the binary64 oracle run of the same
+    configuration (tests/golden/karman_cfg1.npz, made by tests/golden/make_cfg1.py)."""
+    import torch
+
+    from openhomelbm_b200.lbm import LBM_Solver
+
+    torch.cuda.set_device(0)
+    nx, ny, vis, u_in = 512, 128, 0.012, 0.05
+    th = np.linspace(0, 2 * np.pi, 96, endpoint=False)
+    circle = np.stack([np.cos(th), np.sin(th)], 1).astype(np.float32)
+    noise = np.random.default_rng(0).uniform(-1e-3, 1e-3, (nx, ny, 2)).astype(np.float32)
+    m0 = np.zeros((6, nx, ny), np.float32)
+    m0[0] = 1.0
+    m0[1] = np.float32(u_in) + noise[..., 0]
+    m0[2] = noise[..., 1]
+    s = LBM_Solver(nx, ny, solid_num=1)
+    f = s.flows[0]
+    f.vis_shear = vis
+    f.bc_type = [0, 1, 1, 1]
+    f.bc_value = np.array([[u_in, 0.0], [0, 0], [0, 0], [0, 0]], np.float32)
+    t = torch.tensor(m0, device=f.device)
+    f.moments[0].copy_(t)
+    f.moments[1].copy_(t)
+    f.configure_solid(0, circle, (128.0, 64.0), angle=0.0, scale=12.0 / 512.0)
+    steps = args.karman_steps
+    loads = torch.zeros((steps, 2), dtype=torch.float32, device=f.device)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for k in range(steps):
+        s.step()
+        loads[k, 0] = f.solid_forcex[0]
+        loads[k, 1] = f.solid_forcey[0]
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    got = loads.cpu().numpy().astype(np.float64)
+    g = np.load(os.path.join(ROOT, "tests", "golden", "karman_cfg1.npz"))
+    w0, w1 = (int(v) for v in g["window"])
+    ours = shedding_stats(got[w0:w1, 0], got[w0:w1, 1]) if steps >= w1 else None
+    ref = {k: float(g[k]) for k in ("mean_drag", "lift_std", "strouhal", "period_steps")}
+    rel = ({k: ours[k] / ref[k] - 1.0 for k in ("mean_drag", "lift_std", "strouhal")} if ours else None)
+    # CPU baseline: the oracle (C++ restatement of the reference kernels, all host threads)
+    from oracle import oracle as orc
+
+    mr = float(f.solid_max_radius[0].item())
+    sol = orc.Solids2D(line=circle[None], line_num=np.array([96]), position=np.array([[128.0, 64.0]]), angle=np.zeros(1),
+                       scale=np.array([np.float32(12.0 / 512.0)]), mass_center=np.zeros((1, 2)),
+                       max_radius=np.array([mr])).cast(np.float32)
+    flag = orc.border_flags_2d(nx, ny)
+    mm, pp = m0.copy(), m0.copy()
+    threads = orc.max_threads()
+    n_cpu, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < args.cpu_budget:
+        new, _ = orc.step_2d(mm, pp, vis_shear=np.float32(vis), bc_type=[0, 1, 1, 1],
+                             bc_value=[[u_in, 0.0], [0, 0], [0, 0], [0, 0]], flag=flag, solids=sol, nthreads=threads)
+        mm, pp = new, mm
+        n_cpu += 1
+    cpu_s = time.perf_counter() - t0
+    return {"metric": "D2Q9 Karman wake (512x128, Re 100) Strouhal number vs binary64 oracle",
+            "value": ours["strouhal"] if ours else None, "unit": "St", "higher_is_better": None, "n_gpus": 1,
+            "workload": "karman", "steps": steps, "dtype": "f32", "data": "synthetic (seeded inflow noise)",
+            "window": [w0, w1], "ours": ours, "oracle_f64": ref, "relative_difference": rel,
+            "mlups": nx * ny * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
+            "cpu_baseline": {"value": nx * ny * n_cpu / cpu_s / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
+                             "sample": f"{n_cpu} steps of the same 512x128 domain with its cylinder ({cpu_s:.1f} s, "
+                                       "C++ restatement of the reference's D2Q9 kernels, not Warp)"},
+            "config": {"workload": "D2Q9 512x128, 96-gon cylinder r=12 at (128,64), inflow 0.05, nu 0.012, bc 0,1,1,1",
+                       "recorded": "drag (solid_forcex) and lift (solid_forcey) every step, device-side"}}
+
+
 # ----------------------------------------------------------------------------- serving form
 def run_serve(args):
     """The serving form: Poisson arrivals of mesh-coupled D3Q27 domains (sides log-uniform in
@@ -424,6 +510,14 @@ def run_serve(args):
         errs.append(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)))
     cells = sum(r.side ** 3 * r.control_steps * r.substeps for r in reqs)
     sides = [r.side for r in reqs]
+    # accuracy of the served float16 form: final velocity fields against float64 storage (the
+    # same kernels in binary64) for one request of each size up to 160
+    acc_reqs = [serving.Request(100 + k, side, 1000 + k, 0.0, control_steps=args.control_steps)
+                for k, side in enumerate((64, 96, 128, 160))]
+    f64 = serving.ServeEngine(storage="float64", max_active=4, keep_fields=True).run(acc_reqs, realtime=False)
+    f16 = serving.ServeEngine(storage="float16", max_active=4, keep_fields=True).run(acc_reqs, realtime=False)
+    u_l2 = {str(r.side): float(np.linalg.norm(f16.fields[r.rid] - f64.fields[r.rid]) / np.linalg.norm(f64.fields[r.rid]))
+            for r in acc_reqs}
     return {"metric": "served env-steps/s (D3Q27 mesh-coupled domains, float16 storage, continuous batching)",
             "value": served.env_steps_per_s, "unit": "env-steps/s", "higher_is_better": True, "n_gpus": 1,
             "workload": "serve", "dtype": "f32 arithmetic, f16 storage", "data": "synthetic (seeded Poisson requests)",
@@ -435,6 +529,7 @@ def run_serve(args):
             "plain": {"env_steps_per_s": plain.env_steps_per_s, "p50_ms": plain.pct(50) * 1e3,
                       "p99_ms": plain.pct(99) * 1e3, "wall_s": plain.wall_s, "mlups": cells / plain.wall_s / 1e6},
             "loads_rel_l2_f16_vs_plain_f32": {"median": float(np.median(errs)), "max": float(np.max(errs))},
+            "u_l2_f16_vs_f64_by_side": u_l2,
             "config": {"requests": len(reqs), "rate_per_s": args.rate, "control_steps": args.control_steps,
                        "substeps": 8, "slots": args.slots, "hbm_budget_gb": 150,
                        "sides": {str(k): sides.count(k) for k in sorted(set(sides))},
@@ -455,10 +550,11 @@ def main():
     ap.add_argument("--kernel", type=int, default=0, help="0 auto, 1 async-copy kernel, 2 TMA kernel")
     ap.add_argument("--chunks", type=int, default=0, help="x split per tile column (0 automatic)")
     ap.add_argument("--stages", type=int, default=0, help="TMA pipeline stages (0 automatic)")
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "precision", "serve"],
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "precision", "serve", "karman"],
                     help="tgv: the headline throughput line; precision: float64/32/16/bf16 accuracy form; "
                          "serve: served vs plain mesh-coupled domains")
     ap.add_argument("--requests", type=int, default=48, help="serve: number of requests")
+    ap.add_argument("--karman-steps", type=int, default=100000, help="karman: GPU steps")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate (requests/s)")
     ap.add_argument("--control-steps", type=int, default=100, help="serve: control steps per request")
     ap.add_argument("--slots", type=int, default=32, help="serve: concurrently resident domains")
@@ -484,6 +580,8 @@ def main():
             out = run_precision(args) if rank == 0 else None
         elif args.workload == "serve":
             out = run_serve(args) if rank == 0 else None
+        elif args.workload == "karman":
+            out = run_karman(args) if rank == 0 else None
         else:
             out = run_ours(args, rank, world, dist)
         if rank == 0 and out is not None:

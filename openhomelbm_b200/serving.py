@@ -243,6 +243,7 @@ class ServeStats:
     results: Dict[int, np.ndarray]
     max_active: int
     admitted_order: List[int]
+    fields: Dict[int, np.ndarray] = field(default_factory=dict)
 
     @property
     def env_steps_per_s(self) -> float:
@@ -256,19 +257,20 @@ class ServeEngine:
     """Continuous batching of resident domains (see the module docstring)."""
 
     def __init__(self, storage: str = "float16", budget_bytes: float = 150e9, max_active: int = 32,
-                 vis: float = 0.01, device=None):
+                 vis: float = 0.01, device=None, keep_fields: bool = False):
         self.storage = storage
         self.budget = float(budget_bytes)
         self.max_active = int(max_active)
         self.vis = float(vis)
         self.device = _lib.require_cuda(device)
+        self.keep_fields = bool(keep_fields)
 
     def run(self, requests: List[Request], realtime: bool = True) -> ServeStats:
         """Serve the requests (arrival times honoured when ``realtime``) until all finish."""
         pending = sorted(requests, key=lambda r: r.arrival)
         active: List[Domain] = []
         used = 0.0
-        lat, results, order = [], {}, []
+        lat, results, order, fields = [], {}, [], {}
         peak = 0
         steps = 0
         t_start = time.perf_counter()
@@ -313,10 +315,12 @@ class ServeEngine:
             for d in [d for d in active if d.finished]:
                 active.remove(d)
                 results[d.req.rid] = np.stack(d.loads)
+                if self.keep_fields:  # the final velocity field, for accuracy checks
+                    fields[d.req.rid] = d.solver.flows[0].decoded()[1:4].double().cpu().numpy()
                 used -= domain_bytes(d.req.side, self.storage)
                 d.release()
         torch.cuda.synchronize()
-        return ServeStats(steps, time.perf_counter() - t_start, lat, results, peak, order)
+        return ServeStats(steps, time.perf_counter() - t_start, lat, results, peak, order, fields)
 
 
 def run_plain(requests: List[Request], storage: str = "float32", vis: float = 0.01, device=None) -> ServeStats:
