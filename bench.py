@@ -559,6 +559,9 @@ def main():
     ap.add_argument("--control-steps", type=int, default=100, help="serve: control steps per request")
     ap.add_argument("--slots", type=int, default=32, help="serve: concurrently resident domains")
     args = ap.parse_args()
+    if args.workload == "serve":
+        # a hardware work queue per resident domain's stream (before any CUDA call)
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None

@@ -29,6 +29,7 @@
 // bound, lbm_func_3d.py:308). Brute force over the solid's triangles: the band is small and
 // every thread of a warp reads the same triangle, so the loads broadcast.
 
+#include <algorithm>
 #include <cmath>
 
 #include "hl_common.cuh"
@@ -182,9 +183,11 @@ __device__ __forceinline__ bool candidates(const hl_solids3d& s, int k, int ntri
   return *ncand > 0;
 }
 
-// Whether a link of the cell could be cut: some solid within bound_radius + 2 has candidate
-// triangles for rays from the cell.
-template <class R> __device__ bool may_cut(const hl_solids3d& s, V3<R> cell) {
+// The solids whose triangles a link of the cell could hit: within bound_radius + 2 and with
+// candidate triangles for rays from the cell. Bit k for solid k < 32; solids from 32 on are
+// not tracked and are always tested (bit 31 stands for them). Zero: no cut link possible.
+template <class R> __device__ unsigned cut_mask(const hl_solids3d& s, V3<R> cell) {
+  unsigned mask = 0u;
   for (int k = 0; k < s.n_objects; ++k) {
     const int ntri = s.tri_offset[k + 1] - s.tri_offset[k];
     if (ntri == 0) continue;
@@ -196,10 +199,12 @@ template <class R> __device__ bool may_cut(const hl_solids3d& s, V3<R> cell) {
     const R sx = R(s.scale_sizes[3 * k]), sy = R(s.scale_sizes[3 * k + 1]), sz = R(s.scale_sizes[3 * k + 2]);
     const int32_t* list;
     int ncand;
-    if (candidates(s, k, ntri, V3<R>{lo.x / sx, lo.y / sy, lo.z / sz}, sx, sy, sz, &list, &ncand)) return true;
+    if (candidates(s, k, ntri, V3<R>{lo.x / sx, lo.y / sy, lo.z / sz}, sx, sy, sz, &list, &ncand))
+      mask |= k < 31 ? (1u << k) : (1u << 31);
   }
-  return false;
+  return mask;
 }
+__device__ __forceinline__ bool in_mask(unsigned mask, int k) { return (mask >> (k < 31 ? k : 31)) & 1u; }
 
 template <class R> __device__ __forceinline__ R warp_sum(R v) {
 #pragma unroll
@@ -211,7 +216,10 @@ template <class R> __device__ __forceinline__ R warp_sum(R v) {
 // population of direction i (a wall population with its momentum exchange if the link is
 // cut, the clamped neighbour population otherwise), the moments are warp sums, and lane 0
 // collides and stores the cell.
-template <class S> __device__ void cut_cell(const Args& a, double* acc, int x, int y, int z) {
+constexpr int MAXC = 64;  // candidate triangles staged per batch, per warp
+
+template <class S>
+__device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, int z, unsigned mask) {
   using R = typename S::R;
   using T = typename S::T;
   const hl_solids3d& s = a.s;
@@ -221,47 +229,59 @@ template <class S> __device__ void cut_cell(const Args& a, double* acc, int x, i
   const int i = threadIdx.x & 31;
   const Mom3<R> mc = load_cell<S>(a, N, c);
   R pop = R(0);
-  int ix = 0, iy = 0, iz = 0;
-  if (i < 27) {
-    ix = c_cx[i];
-    iy = c_cy[i];
-    iz = c_cz[i];
-    const R dx = R(ix), dy = R(iy), dz = R(iz);
-    const R wi = weight<R>(i);
-    int xn = x - ix, yn = y - iy, zn = z - iz;
-    if (a.w.periodic) {
-      xn = wrap(xn, nx);
-      yn = wrap(yn, ny);
-      zn = wrap(zn, nz);
-    }
-    if (xn >= 0 && xn < nx && yn >= 0 && yn < ny && zn >= 0 && zn < nz) {
-      // get_cutcell_multi_3d: the closest hit in [0, 1] over the solids near the cell
-      R cut = R(-1);
-      int sid = -1;
-      const V3<R> cell{R(x), R(y), R(z)};
-      const V3<R> dir{-dx, -dy, -dz};
-      for (int k = 0; k < s.n_objects; ++k) {
-        const int t0 = s.tri_offset[k], ntri = s.tri_offset[k + 1] - t0;
-        if (ntri == 0) continue;
-        if (vlen(cell.x - R(s.position[3 * k]), cell.y - R(s.position[3 * k + 1]), cell.z - R(s.position[3 * k + 2])) >
-            R(s.bound_radius[k]) + R(2))
-          continue;
-        const Xf<R> inv = xinv(load_xf<R>(s.transforms + 7 * k));
-        const V3<R> lo = xpoint(inv, cell);
-        const V3<R> ld = qrot(inv.qx, inv.qy, inv.qz, inv.qw, dir);
-        const R sx = R(s.scale_sizes[3 * k]), sy = R(s.scale_sizes[3 * k + 1]), sz = R(s.scale_sizes[3 * k + 2]);
-        const V3<R> los{lo.x / sx, lo.y / sy, lo.z / sz};
-        const int32_t* list;
-        int ncand;
-        if (!candidates(s, k, ntri, los, sx, sy, sz, &list, &ncand)) continue;
-        R t;
-        if (ray_mesh<R>(s.tris + 9ll * t0, list, ncand, los, {ld.x / sx, ld.y / sy, ld.z / sz}, R(2), &t)) {
-          if ((cut < R(0) || t < cut) && t >= R(0) && t <= R(1)) {
-            cut = t;
-            sid = k;
-          }
+  const int ix = i < 27 ? c_cx[i] : 0, iy = i < 27 ? c_cy[i] : 0, iz = i < 27 ? c_cz[i] : 0;
+  const R dx = R(ix), dy = R(iy), dz = R(iz);
+  int xn = x - ix, yn = y - iy, zn = z - iz;
+  if (a.w.periodic) {
+    xn = wrap(xn, nx);
+    yn = wrap(yn, ny);
+    zn = wrap(zn, nz);
+  }
+  const bool active = i < 27 && xn >= 0 && xn < nx && yn >= 0 && yn < ny && zn >= 0 && zn < nz;
+  // get_cutcell_multi_3d: the closest hit in [0, 1] over the solids near the cell. Which
+  // solids and which candidate triangles depend on the cell only, so the loop is uniform
+  // across the warp: the warp stages each batch of candidates in shared memory together and
+  // every lane tests its own direction against it.
+  R cut = R(-1);
+  int sid = -1;
+  const V3<R> cell{R(x), R(y), R(z)};
+  const V3<R> dir{-dx, -dy, -dz};
+  for (int k = 0; k < s.n_objects; ++k) {
+    if (!in_mask(mask, k)) continue;  // no candidate triangles for this cell's rays
+    const int t0 = s.tri_offset[k], ntri = s.tri_offset[k + 1] - t0;
+    if (ntri == 0) continue;
+    if (vlen(cell.x - R(s.position[3 * k]), cell.y - R(s.position[3 * k + 1]), cell.z - R(s.position[3 * k + 2])) >
+        R(s.bound_radius[k]) + R(2))
+      continue;
+    const Xf<R> inv = xinv(load_xf<R>(s.transforms + 7 * k));
+    const V3<R> lo = xpoint(inv, cell);
+    const V3<R> ld = qrot(inv.qx, inv.qy, inv.qz, inv.qw, dir);
+    const R sx = R(s.scale_sizes[3 * k]), sy = R(s.scale_sizes[3 * k + 1]), sz = R(s.scale_sizes[3 * k + 2]);
+    const V3<R> los{lo.x / sx, lo.y / sy, lo.z / sz};
+    const int32_t* list;
+    int ncand;
+    if (!candidates(s, k, ntri, los, sx, sy, sz, &list, &ncand)) continue;
+    const float* tk = s.tris + 9ll * t0;
+    for (int b0 = 0; b0 < ncand; b0 += MAXC) {
+      const int m = min(MAXC, ncand - b0);
+      __syncwarp();
+      for (int j = i; j < 9 * m; j += 32) {
+        const int q = b0 + j / 9;
+        buf[j] = tk[9 * (list ? list[q] : q) + j % 9];
+      }
+      __syncwarp();
+      R t;
+      if (active && ray_mesh<R>(buf, nullptr, m, los, {ld.x / sx, ld.y / sy, ld.z / sz}, R(2), &t)) {
+        if ((cut < R(0) || t < cut) && t >= R(0) && t <= R(1)) {
+          cut = t;
+          sid = k;
         }
       }
+    }
+  }
+  if (active) {
+    const R wi = weight<R>(i);
+    {
       if (sid >= 0) {
         const Xf<R> tc = load_xf<R>(s.transforms + 7 * sid);
         const Xf<R> tl = load_xf<R>(s.transforms_last + 7 * sid);
@@ -376,6 +396,7 @@ template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __
   // 1. each lane classifies its cell: fluid, in solid k0's band (and in no lower solid's), and
   //    with candidate triangles for its rays
   int x = 0, y = 0, z = 0;
+  unsigned solids = 0u;
   bool flagged = false;
   if (s.tri_offset[k0 + 1] > s.tri_offset[k0] && isfinite(px) && isfinite(py) && isfinite(pz) && isfinite(r) &&
       idx < (long long)side * side * side) {
@@ -386,9 +407,11 @@ template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __
     const long long c = ((long long)x * ny + y) * nz + z;
     const bool fluid = inside && (a.w.flag == nullptr || a.w.flag[c] == ML_FLUID) &&
                        (a.w.flag != nullptr || a.w.periodic || (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1));
-    flagged = fluid && first_near<R>(s, R(x), R(y), R(z)) == k0 && may_cut<R>(s, V3<R>{R(x), R(y), R(z)});
+    if (fluid && first_near<R>(s, R(x), R(y), R(z)) == k0) solids = cut_mask<R>(s, V3<R>{R(x), R(y), R(z)});
+    flagged = solids != 0u;
   }
   // 2. the warp computes its flagged cells one after another, a lane per direction
+  __shared__ float tri_buf[BLOCK / 32][MAXC * 9];
   unsigned mask = __ballot_sync(0xffffffffu, flagged);
   const bool any = mask != 0;
   while (mask) {
@@ -396,7 +419,8 @@ template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __
     mask &= mask - 1;
     const int cx = __shfl_sync(0xffffffffu, x, src), cy = __shfl_sync(0xffffffffu, y, src),
               cz = __shfl_sync(0xffffffffu, z, src);
-    cut_cell<S>(a, acc, cx, cy, cz);
+    const unsigned cm = __shfl_sync(0xffffffffu, solids, src);
+    cut_cell<S>(a, acc, tri_buf[threadIdx.x >> 5], cx, cy, cz, cm);
     __syncwarp();
   }
   if (!__syncthreads_or(any)) return;
@@ -418,6 +442,7 @@ template <class S> __global__ void __launch_bounds__(BLOCK) classify_kernel(cons
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   bool flagged = false;
   int c = 0;
+  unsigned solids = 0u;
   if (s.tri_offset[k0 + 1] > s.tri_offset[k0] && isfinite(px) && isfinite(py) && isfinite(pz) && isfinite(r) &&
       idx < (long long)side * side * side) {
     const int x = int(floorf(px - r)) + int(idx / ((long long)side * side));
@@ -427,7 +452,8 @@ template <class S> __global__ void __launch_bounds__(BLOCK) classify_kernel(cons
     c = (x * ny + y) * nz + z;
     const bool fluid = inside && (a.w.flag == nullptr || a.w.flag[c] == ML_FLUID) &&
                        (a.w.flag != nullptr || a.w.periodic || (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1));
-    flagged = fluid && first_near<R>(s, R(x), R(y), R(z)) == k0 && may_cut<R>(s, V3<R>{R(x), R(y), R(z)});
+    if (fluid && first_near<R>(s, R(x), R(y), R(z)) == k0) solids = cut_mask<R>(s, V3<R>{R(x), R(y), R(z)});
+    flagged = solids != 0u;
   }
   const unsigned mask = __ballot_sync(0xffffffffu, flagged);
   if (mask == 0) return;
@@ -435,7 +461,11 @@ template <class S> __global__ void __launch_bounds__(BLOCK) classify_kernel(cons
   int base = 0;
   if (lane == leader) base = atomicAdd(s.work, __popc(mask));
   base = __shfl_sync(0xffffffffu, base, leader);
-  if (flagged) s.work[1 + base + __popc(mask & ((1u << lane) - 1))] = c;
+  if (flagged) {
+    const int slot = base + __popc(mask & ((1u << lane) - 1));
+    s.work[2 + 2 * slot] = c;
+    s.work[3 + 2 * slot] = int(solids);
+  }
 }
 
 template <class S> __global__ void __launch_bounds__(BLOCK) process_kernel(const __grid_constant__ Args a) {
@@ -444,14 +474,16 @@ template <class S> __global__ void __launch_bounds__(BLOCK) process_kernel(const
   const int n = s.n_objects;
   for (int k = threadIdx.x; k < 6 * n; k += blockDim.x) acc[k] = 0.0;
   __syncthreads();
+  __shared__ float tri_buf[BLOCK / 32][MAXC * 9];
   const int count = s.work[0];
   const int warps = gridDim.x * (BLOCK / 32);
   const int ny = a.w.ny, nz = a.w.nz;
   bool any = false;
   for (int j = blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5); j < count; j += warps) {
-    const int c = s.work[1 + j];
+    const int c = s.work[2 + 2 * j];
+    const unsigned cm = unsigned(s.work[3 + 2 * j]);
     any = true;
-    cut_cell<S>(a, acc, c / (ny * nz), (c / nz) % ny, c % nz);
+    cut_cell<S>(a, acc, tri_buf[threadIdx.x >> 5], c / (ny * nz), (c / nz) % ny, c % nz, cm);
     __syncwarp();
   }
   if (!__syncthreads_or(any)) return;
@@ -497,6 +529,8 @@ template <class S> int launch(const hl_world3d* w, double vis, const hl_solids3d
     if (e != cudaSuccess) return cuda_status(e, "d3q27 solid links: zero work count");
     classify_kernel<S><<<grid, BLOCK, 0, st>>>(a);
     HL_LAUNCH_CHECK("d3q27 solid links (classify)");
+    // four blocks per SM take the listed cells in turn (measured: smaller grids leave the
+    // densely listed bands of small domains to too few warps)
     process_kernel<S><<<unsigned(4 * num_sms_local()), BLOCK, 0, st>>>(a);
     HL_LAUNCH_CHECK("d3q27 solid links (cut cells)");
   } else {
@@ -542,5 +576,5 @@ extern "C" int hl_d3q27_solid_links(const hl_world3d* w, double vis_shear, const
 extern "C" size_t hl_d3q27_solid_links_work_ints(int n_objects, float max_bound_radius) {
   if (n_objects <= 0 || !(max_bound_radius >= 0.f) || max_bound_radius >= 512.f) return 0;
   const size_t side = size_t(d3s::box_side_of(max_bound_radius));
-  return 1 + size_t(n_objects) * side * side * side;
+  return 2 + 2 * size_t(n_objects) * side * side * side;  // count, pad, then (cell, solid mask) pairs
 }

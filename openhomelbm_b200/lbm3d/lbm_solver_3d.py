@@ -184,7 +184,9 @@ class LBM_Solver3D:
         return any(t is not None and len(t) for t in self._mesh_tris)
 
     # ------------------------------------------------------------------ stepping
-    def _launch(self, parity: int, stream) -> None:
+    def _launch(self, parity: int, stream, loads_out=None) -> None:
+        """One step of every world on ``stream``. ``loads_out`` (optional, per world a pair of
+        device pointers) redirects the binary32 solid force / torque [n][3] of the step."""
         L = _lib.lib()
         meshes = self.has_meshes
         for k, f in enumerate(self.flows):
@@ -195,7 +197,10 @@ class LBM_Solver3D:
                                     self.mass[k:k + 1].data_ptr(), self.health[k:k + 1].data_ptr())
             _lib.check(L.hl_d3q27_stream_collide(w, float(f.vis_shear), diag, stream), "stream_and_collide_3d")
             if meshes:
-                _lib.check(L.hl_d3q27_solid_links(w, float(f.vis_shear), self._solids_struct(k), stream),
+                sst = self._solids_struct(k)
+                if loads_out is not None:
+                    sst.force, sst.torque = loads_out[k]
+                _lib.check(L.hl_d3q27_solid_links(w, float(f.vis_shear), sst, stream),
                            "stream_and_collide_3d (cut links)")
             if not f.periodic:
                 _lib.check(L.hl_d3q27_apply_bc(w, f.bc_struct(), _lib.ptr(self._bc_scratch[k]), stream),

@@ -22,6 +22,7 @@ read and write only that domain's buffers.
 from __future__ import annotations
 
 import math
+import os
 import time
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Tuple
@@ -33,6 +34,10 @@ from . import _lib
 from .lbm3d import LBM_Solver3D
 
 SEGMENTS = 5
+# One hardware work queue per domain stream: with CUDA's default of 8, the streams of more
+# than 8 domains share queues and their graphs run one after another. Effective only when
+# this module is imported before the process creates its CUDA context.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 
 # ----------------------------------------------------------------------------- bodies
@@ -90,15 +95,20 @@ class Swimmer:
 
     def poses(self, t: float) -> Tuple[np.ndarray, np.ndarray]:
         """Joint positions (SEGMENTS, 3) and orientations (SEGMENTS, 4) as (w, x, y, z)."""
-        pos = np.zeros((SEGMENTS, 3))
-        quat = np.zeros((SEGMENTS, 4))
-        p = self.head.astype(np.float64).copy()
-        yaw = 0.0
-        for k in range(SEGMENTS):
-            yaw += self.amp[k] * math.sin(2 * math.pi * self.freq * t + self.phase[k])
-            pos[k] = p
-            quat[k] = (math.cos(yaw / 2), 0.0, 0.0, math.sin(yaw / 2))
-            p = p + self.seg_len * np.array([math.cos(yaw), math.sin(yaw), 0.0])
+        pos, quat = self.poses_at(np.array([t], np.float64))
+        return pos[0], quat[0]
+
+    def poses_at(self, ts: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+        """Poses at every time of ``ts``: positions (T, SEGMENTS, 3), quaternions (T, SEGMENTS, 4).
+        Segment k's yaw is the sum of joint angles 0..k; joint k + 1 sits one segment length
+        along segment k's axis."""
+        ts = np.asarray(ts, np.float64)
+        ang = self.amp[None, :] * np.sin(2 * np.pi * self.freq * ts[:, None] + self.phase[None, :])
+        yaw = np.cumsum(ang, axis=1)
+        step = self.seg_len * np.stack([np.cos(yaw), np.sin(yaw), np.zeros_like(yaw)], axis=2)
+        pos = self.head[None, None, :] + np.concatenate([np.zeros_like(step[:, :1]), np.cumsum(step, axis=1)[:, :-1]],
+                                                          axis=1)
+        quat = np.stack([np.cos(yaw / 2), np.zeros_like(yaw), np.zeros_like(yaw), np.sin(yaw / 2)], axis=2)
         return pos.astype(np.float32), quat.astype(np.float32)
 
 
@@ -164,8 +174,9 @@ class Domain:
             self.pos_dev = torch.zeros((S, SEGMENTS, 3), dtype=torch.float32, device=dev)
             self.quat_dev = torch.zeros((S, SEGMENTS, 4), dtype=torch.float32, device=dev)
             self.buf = 0
-            self.loads_dev = torch.zeros((S, SEGMENTS, 6), dtype=torch.float32, device=dev)
-            self.loads_host = torch.zeros((S, SEGMENTS, 6), dtype=torch.float32).pin_memory()
+            # loads of every substep, written by the cut-link pass itself: [substep][force, torque][segment][3]
+            self.loads_dev = torch.zeros((S, 2, SEGMENTS, 3), dtype=torch.float32, device=dev)
+            self.loads_host = torch.zeros((S, 2, SEGMENTS, 3), dtype=torch.float32).pin_memory()
             self.ids = torch.arange(SEGMENTS, dtype=torch.int32, device=dev)
             self.zeros3 = torch.zeros((SEGMENTS, 3), dtype=torch.float32, device=dev)
             self.ones = torch.ones(SEGMENTS, dtype=torch.float32, device=dev)
@@ -179,12 +190,11 @@ class Domain:
 
     def _control_step(self) -> None:
         """One control step on the current stream: per substep, the swimmer's pose from the
-        pose buffer (convert_and_update_solid_batch_3d), one LBM step with the cut links, and
-        a copy of the segments' loads."""
+        pose buffer (convert_and_update_solid_batch_3d) and one LBM step with the cut links,
+        whose loads go straight to the substep's slot of the load buffer."""
         s = self.solver
         L = _lib.lib()
         st = _lib.stream_ptr()
-        f = s.flows[0]
         for k in range(self.req.substeps):
             _lib.check(L.hl_couple3d_update_solids(
                 1, SEGMENTS, SEGMENTS, _lib.ptr(self.ids), self.pos_dev[k].data_ptr(), self.quat_dev[k].data_ptr(),
@@ -192,19 +202,16 @@ class Domain:
                 _lib.ptr(s.solid_position_all), _lib.ptr(s.solid_quaternion_all), _lib.ptr(s.mesh_transforms_all),
                 _lib.ptr(s.mesh_transforms_last_all), _lib.ptr(s.mesh_transforms_initialized_all), st),
                 "pose update")
-            s._launch(k % 2, st)
-            self.loads_dev[k, :, :3].copy_(f.solid_force)
-            self.loads_dev[k, :, 3:].copy_(f.solid_torque)
+            s._launch(k % 2, st, loads_out=[(self.loads_dev[k, 0].data_ptr(), self.loads_dev[k, 1].data_ptr())])
 
     def stage_poses(self, step: int) -> None:
         """Host: the swimmer's poses for every substep of control step ``step``, into the host
         buffer that the launch of that step uploads."""
         S = self.req.substeps
         buf = step % 2
-        for k in range(S):
-            pos, quat = self.swimmer.poses(step * S + k + 1)
-            self.pos_host[buf][k] = torch.from_numpy(pos)
-            self.quat_host[buf][k] = torch.from_numpy(quat)
+        pos, quat = self.swimmer.poses_at(np.arange(step * S + 1, step * S + S + 1))
+        self.pos_host[buf].numpy()[...] = pos
+        self.quat_host[buf].numpy()[...] = quat
 
     def launch(self) -> None:
         """Enqueue the next control step on the domain's stream (pose upload, the step, the
@@ -221,7 +228,8 @@ class Domain:
             self.event.record(self.stream)
 
     def finish(self, latency: float) -> None:
-        self.loads.append(self.loads_host.numpy().copy())
+        # per substep and segment: force then torque (the plain baseline's layout)
+        self.loads.append(np.concatenate([self.loads_host[:, 0].numpy(), self.loads_host[:, 1].numpy()], axis=2))
         self.latencies.append(latency)
         self.done += 1
 
@@ -380,10 +388,9 @@ class PlainDomain:
 
         s, S = self.solver, self.req.substeps
         t0 = self.done * S
-        for k in range(S):
-            pos, quat = self.swimmer.poses(t0 + k + 1)
-            self.pos_host[k, 0] = torch.from_numpy(pos)
-            self.quat_host[k, 0] = torch.from_numpy(quat)
+        pos, quat = self.swimmer.poses_at(np.arange(t0 + 1, t0 + S + 1))
+        self.pos_host.numpy()[:, 0] = pos
+        self.quat_host.numpy()[:, 0] = quat
         self.pos_dev.copy_(self.pos_host, non_blocking=True)
         self.quat_dev.copy_(self.quat_host, non_blocking=True)
         f = s.flows[0]
