@@ -536,6 +536,69 @@ def run_serve(args):
                        "triangles_per_body": 1800, "segments": serving.SEGMENTS}}
 
 
+def run_batch(args):
+    """The batching form: args.worlds D2Q9 worlds (nx ~ logU[256, 1024], ny ~ logU[128, 512] from
+    default_rng(args.seed)), each with an 8-capsule swimmer (body 64 cells, capsule radius 4) on
+    a prescribed travelling wave, float16 storage, 8 substeps per control step. A substep is one
+    launch per phase for all worlds, the stream phase one persistent launch over the tile
+    work-list (tile shape and grid from the autotuner); a control step is one CUDA graph. The
+    same worlds one at a time through the plain float32 solver are the baseline. The tile
+    kernel is also timed alone (stream phase of all worlds, CUDA events; the batch's fields,
+    ~10 M cells x 24 B, exceed L2) for its HBM roofline: 24 B per cell update (6 float16
+    moments read and written)."""
+    import torch
+
+    from openhomelbm_b200 import _lib, batching
+
+    torch.cuda.set_device(0)
+    specs = batching.swimmer_specs(args.worlds, seed=args.seed)
+    tuner = batching.TileAutotuner()
+    sb = batching.SwimmerBatch2D(specs, storage="float16", autotuner=tuner)
+    sb.run(2)  # warm-up
+    K = args.batch_control_steps
+    stats = sb.run(K)
+    b, st = sb.batch, _lib.stream_ptr()
+    reps = 50
+    for _ in range(5):
+        b.launch(0, st, phases=_lib.HL_PHASE_STREAM, any_solid=False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        b.launch(0, st, phases=_lib.HL_PHASE_STREAM, any_solid=False)
+    e1.record()
+    torch.cuda.synchronize()
+    t_kernel = e0.elapsed_time(e1) / reps * 1e-3
+    cells = b.cells()
+    achieved = cells * 24 / t_kernel / 1e9
+    peak, peak_kind = measured_peaks()
+    # the plain run covers the batch's warm-up control steps too; compare the same steps
+    plain = batching.run_sequential_plain(specs, K + 2)
+    a, p = stats.loads.astype(np.float64), plain.loads[2:].astype(np.float64)
+    rel = float(np.linalg.norm(a - p) / np.linalg.norm(p))
+    cfg = stats.config
+    table = {f"{c.tile_x}x{c.tile_y}/{c.ctas}": round(ms * 1e3, 1) for c, ms in sorted(stats.tune_table.items(),
+                                                                                       key=lambda kv: kv[1])}
+    return {"metric": "batched MLUPS (uneven D2Q9 worlds with capsule swimmers, float16 storage)",
+            "value": stats.mlups, "unit": "MLUPS", "higher_is_better": True, "n_gpus": 1, "workload": "batch",
+            "dtype": "f32 arithmetic, f16 storage", "data": "synthetic (seeded sizes and swimmers)",
+            "vs_sequential": stats.mlups / plain.mlups,
+            "batched": {"mlups": stats.mlups, "ms_per_control_step": stats.wall_s / K * 1e3,
+                        "p50_ms": float(np.percentile(stats.latencies_s, 50)) * 1e3,
+                        "p99_ms": float(np.percentile(stats.latencies_s, 99)) * 1e3,
+                        "tile": [cfg.tile_x, cfg.tile_y], "ctas": cfg.ctas},
+            "sequential_plain": {"mlups": plain.mlups,
+                                 "ms_per_control_step_all_worlds": plain.wall_s / (K + 2) * 1e3},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "kernel": "stream_tiles_kernel",
+                         "us_per_launch": t_kernel * 1e6, "bytes_per_cell": 24},
+            "autotuner_us_per_launch": table,
+            "loads_rel_l2_f16_batch_vs_plain_f32": rel,
+            "config": {"workload": "batch", "worlds": len(specs), "seed": args.seed, "cells": cells,
+                       "control_steps": K, "substeps": 8, "capsules": 8, "storage": "float16",
+                       "l2": "inputs larger than L2"}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -550,9 +613,13 @@ def main():
     ap.add_argument("--kernel", type=int, default=0, help="0 auto, 1 async-copy kernel, 2 TMA kernel")
     ap.add_argument("--chunks", type=int, default=0, help="x split per tile column (0 automatic)")
     ap.add_argument("--stages", type=int, default=0, help="TMA pipeline stages (0 automatic)")
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "precision", "serve", "karman"],
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "precision", "serve", "karman", "batch"],
                     help="tgv: the headline throughput line; precision: float64/32/16/bf16 accuracy form; "
-                         "serve: served vs plain mesh-coupled domains")
+                         "serve: served vs plain mesh-coupled domains; karman: D2Q9 wake vs the oracle; "
+                         "batch: uneven D2Q9 worlds in one persistent launch vs sequential plain solves")
+    ap.add_argument("--worlds", type=int, default=64, help="batch: number of worlds")
+    ap.add_argument("--seed", type=int, default=0, help="batch: seed of the world sizes and swimmers")
+    ap.add_argument("--batch-control-steps", type=int, default=20, help="batch: timed control steps")
     ap.add_argument("--requests", type=int, default=48, help="serve: number of requests")
     ap.add_argument("--karman-steps", type=int, default=100000, help="karman: GPU steps")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate (requests/s)")
@@ -585,6 +652,8 @@ def main():
             out = run_serve(args) if rank == 0 else None
         elif args.workload == "karman":
             out = run_karman(args) if rank == 0 else None
+        elif args.workload == "batch":
+            out = run_batch(args) if rank == 0 else None
         else:
             out = run_ours(args, rank, world, dist)
         if rank == 0 and out is not None:

@@ -335,6 +335,23 @@ HL_API int hl_d2q9_pack(const hl_world2d* w, const hl_step2d* p, const hl_bc2d* 
 HL_API int hl_d2q9_step_batch(const void* desc_dev, int n_worlds, int parity, hl_dtype dtype, int max_nx,
                        int max_ny, int any_solid, int phases, hl_stream stream);
 
+/* Batching form: the stream phase of batched worlds of different sizes as ONE persistent
+ * launch over a tile work-list (no reference counterpart; it replaces the per-world
+ * stream_and_collide launches of LBM_Solver.step, lbm_solver.py:117-139, for uneven worlds).
+ * hl_d2q9_tile_shapes writes the supported tile shapes (tile_x, tile_y pairs, at most cap)
+ * and returns their number. hl_d2q9_tile_list (host only, no GPU) writes the tiles of n_worlds
+ * worlds of nx[w] x ny[w] cells, world-major, 4 int32 per tile (world, x0, y0, 0), into out
+ * (NULL: count only) and their number into *n_tiles; HL_ERR_ARG if they do not fit in
+ * cap_tiles. hl_d2q9_step_tiles runs hl_d2q9_step_batch's phases with the stream phase taken
+ * by min(n_tiles, ctas) CTAs that take the tiles in turn; tiles_dev (device, 16-byte aligned)
+ * holds the list for the same tile shape. Results are identical to hl_d2q9_step_batch. */
+HL_API int hl_d2q9_tile_shapes(int32_t* out, int cap);
+HL_API int hl_d2q9_tile_list(const int32_t* nx, const int32_t* ny, int n_worlds, int tile_x, int tile_y, int32_t* out,
+                             size_t cap_tiles, size_t* n_tiles);
+HL_API int hl_d2q9_step_tiles(const void* desc_dev, int n_worlds, int parity, hl_dtype dtype, const int32_t* tiles_dev,
+                              int n_tiles, int tile_x, int tile_y, int ctas, int any_solid, int phases,
+                              hl_stream stream);
+
 /* Replaces InitFlow (envs/lbm/lbm_func.py:26-63) and set_uniform_flow_kernel
  * (envs/lbm/karman/karman_lbm_env.py:15-53), both buffers. fx/fy may be NULL. */
 HL_API int hl_d2q9_init_uniform(int nx, int ny, hl_storage storage, void* m_a, void* m_b, float* fx, float* fy,

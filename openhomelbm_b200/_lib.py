@@ -104,6 +104,10 @@ _SIGS = {
     "hl_d2q9_pack": ([POINTER(hl_world2d), POINTER(hl_step2d), POINTER(hl_bc2d), POINTER(hl_solids2d),
                       c_void_p], c_int),
     "hl_d2q9_step_batch": ([c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p], c_int),
+    "hl_d2q9_tile_shapes": ([c_void_p, c_int], c_int),
+    "hl_d2q9_tile_list": ([c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_size_t, POINTER(c_size_t)], c_int),
+    "hl_d2q9_step_tiles": ([c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int, c_int, c_int, c_int, c_int,
+                            c_void_p], c_int),
     "hl_d2q9_init_uniform": ([c_int, c_int, hl_storage, c_void_p, c_void_p, c_void_p, c_void_p, c_float,
                               c_float, c_void_p], c_int),
     "hl_d2q9_init_boundary": ([c_int, c_int, c_void_p, c_void_p], c_int),

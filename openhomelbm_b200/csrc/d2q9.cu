@@ -33,9 +33,14 @@ template <class R> __device__ __forceinline__ R w2(int i) { return i == 0 ? R(4.
 // mlCalDistribution (envs/lbm/lbm_func.py:685-788): population i rebuilt from (rho, u, S)
 // with the third-order Hermite terms Axxy, Axyy, returned as the deviation f_i - w_i
 // (the reference's bracket minus one: w_i (rho - 1 + rho (bracket_i - 1))).
-template <class R> __device__ __forceinline__ R feq_dev(const Mom2<R>& m, int i) {
-  const R Axxy = m.sxx * m.uy + R(2) * m.sxy * m.ux - R(2) * m.ux * m.ux * m.uy;
-  const R Axyy = m.syy * m.ux + R(2) * m.sxy * m.uy - R(2) * m.ux * m.uy * m.uy;
+template <class R> __device__ __forceinline__ R third_xxy(const Mom2<R>& m) {
+  return m.sxx * m.uy + R(2) * m.sxy * m.ux - R(2) * m.ux * m.ux * m.uy;
+}
+template <class R> __device__ __forceinline__ R third_xyy(const Mom2<R>& m) {
+  return m.syy * m.ux + R(2) * m.sxy * m.uy - R(2) * m.ux * m.uy * m.uy;
+}
+// The same with the third-order terms Axxy = third_xxy(m), Axyy = third_xyy(m) given.
+template <class R> __device__ __forceinline__ R feq_dev_a(const Mom2<R>& m, R Axxy, R Axyy, int i) {
   const R h = R(1.5);
   R b;
   switch (i) {
@@ -51,10 +56,16 @@ template <class R> __device__ __forceinline__ R feq_dev(const Mom2<R>& m, int i)
   }
   return w2<R>(i) * (m.drho + m.rho * b);
 }
+template <class R> __device__ __forceinline__ R feq_dev(const Mom2<R>& m, int i) {
+  return feq_dev_a<R>(m, third_xxy<R>(m), third_xyy<R>(m), i);
+}
 
 // The clamped deviation: f_i >= 0 is f_i - w_i >= -w_i (lbm_func.py:411-412).
 template <class R> __device__ __forceinline__ R feq_dev_clamped(const Mom2<R>& m, int i) {
   return fmax(feq_dev<R>(m, i), -w2<R>(i));
+}
+template <class R> __device__ __forceinline__ R feq_dev_clamped_a(const Mom2<R>& m, R Axxy, R Axyy, int i) {
+  return fmax(feq_dev_a<R>(m, Axxy, Axyy, i), -w2<R>(i));
 }
 
 // Moment-space collision of stream_and_collide (envs/lbm/lbm_func.py:414-467) from deviation
@@ -154,6 +165,8 @@ __device__ __forceinline__ bool is_fluid(const World& w, int x, int y, long long
 // -------------------------------------------------------------------------- 1. prologue
 __global__ void prologue_kernel(const __grid_constant__ Launch L) {
   const World& w = world_of(L, blockIdx.x);
+  // a world of the batch without solids has no solid buffers (box, loads64 NULL)
+  if (w.n_objects == 0 || w.box == nullptr) return;
   __shared__ int box[4];
   if (threadIdx.x == 0) {
     box[0] = w.nx;
@@ -236,6 +249,108 @@ template <class S> __global__ void __launch_bounds__(256) stream_kernel(const __
   store2<S>(w, N, c, static_cast<T*>(post_of(L, w)), collide<R>(pop, Fx, Fy, omega_of<R>(w.vis_shear)));
 }
 
+// ------------------------------------------------------------- 2b. stream over a tile work-list
+// The stream phase of batched worlds of different sizes as one persistent launch: the CTAs of
+// a fixed grid take the tiles of a work list in turn (tile t = {world, x0, y0, 0}, TX x TY
+// cells, clipped to the world). A CTA decodes the tile's moments and a one-cell halo into
+// shared memory (each moment plane read in coalesced rows along y), then computes every fluid
+// cell of the tile from there. The arithmetic is stream_kernel's (feq_dev_clamped, collide on
+// the same decoded moments), so the results are identical to it.
+constexpr int TILE_THREADS = 256;
+constexpr int MOM2_WORDS = 9;  // rho, drho, ux, uy, sxx, syy, sxy, Axxy, Axyy
+
+template <int TX, int TY, class R> constexpr size_t tile_smem_bytes() {
+  return size_t(TX + 2) * (TY + 2) * MOM2_WORDS * sizeof(R);
+}
+
+template <class S, int TX, int TY>
+__global__ void __launch_bounds__(TILE_THREADS) stream_tiles_kernel(const __grid_constant__ Launch L,
+                                                                    const int4* __restrict__ tiles, int n_tiles) {
+  using R = typename S::R;
+  using T = typename S::T;
+  constexpr int HY = TY + 2, HC = (TX + 2) * HY;
+  extern __shared__ __align__(16) unsigned char tile_smem[];
+  R* sm = reinterpret_cast<R*>(tile_smem);  // [HC][9] decoded moments (and third-order terms)
+  for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    const int4 tile = tiles[t];
+    // the world's fields in registers: reads through the descriptor could not be kept across
+    // the stores to post
+    const World& wd = world_of(L, tile.x);
+    const int nx = wd.nx, ny = wd.ny;
+    const bool periodic = wd.periodic != 0;
+    const int* __restrict__ flag = wd.flag;
+    const float* __restrict__ fxp = wd.fx;
+    const float* __restrict__ fyp = wd.fy;
+    const Scale sc = wd.sc;
+    const T* __restrict__ cur = static_cast<const T*>(cur_of(L, wd));
+    T* __restrict__ post = static_cast<T*>(post_of(L, wd));
+    const R omega = omega_of<R>(wd.vis_shear);
+    const int x0 = tile.y, y0 = tile.z;
+    const long long N = (long long)nx * ny;
+    __syncthreads();  // the previous tile's cells are done with the staged moments
+    for (int h = threadIdx.x; h < HC; h += TILE_THREADS) {
+      int gx = x0 - 1 + h / HY, gy = y0 - 1 + h % HY;
+      if (periodic) {
+        gx = wrap(gx, nx);
+        gy = wrap(gy, ny);
+      }
+      if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) {
+        const long long i = (long long)gx * ny + gy;
+        R raw[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) raw[k] = S::to_r(cur[k * N + i]);
+        const Mom2<R> m = decode2<S>(raw, sc);
+        R* d = sm + h * MOM2_WORDS;
+        d[0] = m.rho;
+        d[1] = m.drho;
+        d[2] = m.ux;
+        d[3] = m.uy;
+        d[4] = m.sxx;
+        d[5] = m.syy;
+        d[6] = m.sxy;
+        d[7] = third_xxy<R>(m);
+        d[8] = third_xyy<R>(m);
+      }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < TX * TY; c += TILE_THREADS) {
+      const int lx = c / TY, ly = c % TY;
+      const int x = x0 + lx, y = y0 + ly;
+      if (x >= nx || y >= ny) continue;
+      const long long ci = (long long)x * ny + y;
+      if (flag ? flag[ci] != ML_FLUID : !periodic && !(x > 0 && x < nx - 1 && y > 0 && y < ny - 1)) continue;
+      R pop[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {
+        int xn = x - cx_of(i), yn = y - cy_of(i);
+        if (periodic) {
+          xn = wrap(xn, nx);
+          yn = wrap(yn, ny);
+        }
+        if (xn >= 0 && xn < nx && yn >= 0 && yn < ny) {
+          const R* q = sm + ((lx + 1 - cx_of(i)) * HY + (ly + 1 - cy_of(i))) * MOM2_WORDS;
+          Mom2<R> m;
+          m.rho = q[0];
+          m.drho = q[1];
+          m.ux = q[2];
+          m.uy = q[3];
+          m.sxx = q[4];
+          m.syy = q[5];
+          m.sxy = q[6];
+          pop[i] = feq_dev_clamped_a<R>(m, q[7], q[8], i);
+        } else {
+          pop[i] = -w2<R>(i);  // out of range: f = 0
+        }
+      }
+      const R Fx = fxp ? R(fxp[ci]) : R(0), Fy = fyp ? R(fyp[ci]) : R(0);
+      R raw[6];
+      encode2<S>(collide<R>(pop, Fx, Fy, omega), sc, raw);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) post[k * N + ci] = S::from_r(raw[k]);
+    }
+  }
+}
+
 // -------------------------------------------------------------------------- 3. band
 struct Cut {
   float t, ratio;
@@ -273,10 +388,43 @@ __device__ Cut get_cutcell(const World& w, float x, float y, float dx, float dy)
   return r;
 }
 
+// get_cutcell over a candidate list: cand[k] = (solid << 16) | segment, in ascending
+// (solid, segment) order, holding every segment of a near solid that can cross a link of the
+// cell. The per-segment arithmetic and the tie rule (first nearest wins) are get_cutcell's, so
+// the result is the same.
+__device__ Cut get_cutcell_list(const World& w, const int* cand, int nc, float x, float y, float dx, float dy) {
+  Cut r{-1.f, -1.f, -1, -1};
+  const float ax = x - dx, ay = y - dy, bx = x, by = y;
+  for (int k = 0; k < nc; ++k) {
+    const int s = cand[k] >> 16, n = cand[k] & 0xffff;
+    const int nseg = w.line_num[s];
+    const float* tf = w.tf + size_t(s) * w.max_segments * 2;
+    const int n1 = n + 1 == nseg ? 0 : n + 1;
+    const float cx = tf[2 * n], cy = tf[2 * n + 1], ex = tf[2 * n1], ey = tf[2 * n1 + 1];
+    const float abc = (ax - cx) * (by - cy) - (ay - cy) * (bx - cx);
+    const float abd = (ax - ex) * (by - ey) - (ay - ey) * (bx - ex);
+    if (abc * abd >= 0.f) continue;
+    const float cda = (cx - ax) * (ey - ay) - (cy - ay) * (ex - ax);
+    const float cdb = cda + abc - abd;
+    if (cda * cdb > 0.f) continue;
+    const float t = 1.f - cda / (abd - abc);
+    if (r.t < 0.f || t < r.t) {
+      r.t = t;
+      r.solid = s;
+      r.ratio = abc / (abc - abd);
+      r.seg = n;
+    }
+  }
+  return r;
+}
+
+constexpr int MAX_CAND = 24;  // candidate segments kept per cell; more: the full scan
+
 template <class S> __global__ void __launch_bounds__(256) band_kernel(const __grid_constant__ Launch L) {
   using R = typename S::R;
   using T = typename S::T;
   const World& w = world_of(L, blockIdx.y);
+  if (w.n_objects == 0 || w.box == nullptr) return;  // a world of the batch without solids
   __shared__ double acc[MAX_SOLIDS * 3];
   __shared__ int touched;
   const int nsol = min(w.n_objects, MAX_SOLIDS);
@@ -294,13 +442,34 @@ template <class S> __global__ void __launch_bounds__(256) band_kernel(const __gr
       const int x = x0 + int(k / bw), y = y0 + int(k % bw);
       const long long c = (long long)x * w.ny + y;
       if (!is_fluid(w, x, y, c)) continue;
-      bool near = false;
-      for (int s = 0; s < w.n_objects && !near; ++s) {
-        const float px = float(x) - w.position[2 * s], py = float(y) - w.position[2 * s + 1];
+      // The segments of the near solids (get_cutcell's radius test) that can cross a link of
+      // this cell: every link lies in the square [x-1, x+1] x [y-1, y+1], so a segment whose
+      // box misses that square widened by 1e-3 crosses none. No candidate: no cut link, and
+      // the stream kernel's value is already the cell's update.
+      int cand[MAX_CAND];
+      int nc = 0;
+      bool overflow = false;
+      const float fxc = float(x), fyc = float(y);
+      for (int s = 0; s < w.n_objects; ++s) {
+        const int nseg = w.line_num[s];
+        if (nseg <= 0) continue;
+        const float px = fxc - w.position[2 * s], py = fyc - w.position[2 * s + 1];
         const float scale = w.scale[s] * float(w.nx);
-        near = w.line_num[s] > 0 && px * px + py * py <= w.max_radius[s] * scale * scale;
+        if (px * px + py * py > w.max_radius[s] * scale * scale) continue;
+        const float* tf = w.tf + size_t(s) * w.max_segments * 2;
+        for (int n = 0; n < nseg; ++n) {
+          const int n1 = n + 1 == nseg ? 0 : n + 1;
+          const float cx = tf[2 * n], cy = tf[2 * n + 1], ex = tf[2 * n1], ey = tf[2 * n1 + 1];
+          if (fmaxf(cx, ex) < fxc - 1.001f || fminf(cx, ex) > fxc + 1.001f || fmaxf(cy, ey) < fyc - 1.001f ||
+              fminf(cy, ey) > fyc + 1.001f)
+            continue;
+          if (nc < MAX_CAND)
+            cand[nc++] = (s << 16) | n;
+          else
+            overflow = true;
+        }
       }
-      if (!near) continue;
+      if (nc == 0) continue;
       const Mom2<R> me = load2<S>(w, N, c, cur);
       R pop[9];
       bool any_cut = false;
@@ -313,7 +482,8 @@ template <class S> __global__ void __launch_bounds__(256) band_kernel(const __gr
         }
         pop[i] = -w2<R>(i);
         if (!(xn >= 0 && xn < w.nx && yn >= 0 && yn < w.ny)) continue;
-        const Cut cc = get_cutcell(w, float(x), float(y), float(cx_of(i)), float(cy_of(i)));
+        const Cut cc = overflow ? get_cutcell(w, fxc, fyc, float(cx_of(i)), float(cy_of(i)))
+                                : get_cutcell_list(w, cand, nc, fxc, fyc, float(cx_of(i)), float(cy_of(i)));
         if (cc.t >= 0.f && cc.solid >= 0) {
           any_cut = true;
           const int s = cc.solid, nseg = w.line_num[s];
@@ -537,7 +707,8 @@ int fill_world(const hl_world2d* w, const hl_step2d* p, const hl_bc2d* bc, const
   }
   if (s && s->n_objects > 0) {
     HL_CHECK_ARG(s->n_objects <= d2::MAX_SOLIDS, "d2q9: at most %d solids per world", d2::MAX_SOLIDS);
-    HL_CHECK_ARG(s->max_segments > 0, "d2q9: max_segments must be positive");
+    HL_CHECK_ARG(s->max_segments > 0 && s->max_segments < 65536, "d2q9: max_segments %d out of range (1..65535)",
+                 s->max_segments);
     HL_CHECK_ARG(s->line && s->line_num && s->line_tf && s->line_tf_last && s->position && s->angle && s->scale &&
                      s->mass_center && s->max_radius && s->loads64 && s->band_box,
                  "d2q9: incomplete solid description");
@@ -562,16 +733,57 @@ int fill_world(const hl_world2d* w, const hl_step2d* p, const hl_bc2d* bc, const
   return HL_OK;
 }
 
+// The tile shapes of the persistent stream launch (cells along x, along y).
+constexpr int TILE_SHAPES[][2] = {{8, 32}, {16, 32}, {4, 64}, {8, 64}, {16, 64}, {8, 128}};
+constexpr int N_TILE_SHAPES = int(sizeof(TILE_SHAPES) / sizeof(TILE_SHAPES[0]));
+
+// A tile work-list for the stream phase (NULL: the gridded stream_kernel).
+struct TileWork {
+  const int4* tiles;
+  int n_tiles, tile_x, tile_y, ctas;
+};
+
+template <class S, int TX, int TY> int launch_tiles(const d2::Launch& L, const TileWork& tw, cudaStream_t st) {
+  auto kern = d2::stream_tiles_kernel<S, TX, TY>;
+  const size_t smem = d2::tile_smem_bytes<TX, TY, typename S::R>();
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return cuda_status(e, "d2q9 tiles: shared memory size");
+  }
+  const int grid = tw.n_tiles < tw.ctas ? tw.n_tiles : tw.ctas;
+  kern<<<grid, d2::TILE_THREADS, smem, st>>>(L, tw.tiles, tw.n_tiles);
+  HL_LAUNCH_CHECK("d2q9 stream_and_collide (tile work-list)");
+  return HL_OK;
+}
+
+template <class S> int stream_tiles(const d2::Launch& L, const TileWork& tw, cudaStream_t st) {
+  if (tw.n_tiles == 0) return HL_OK;
+  const int x = tw.tile_x, y = tw.tile_y;
+  if (x == 8 && y == 32) return launch_tiles<S, 8, 32>(L, tw, st);
+  if (x == 16 && y == 32) return launch_tiles<S, 16, 32>(L, tw, st);
+  if (x == 4 && y == 64) return launch_tiles<S, 4, 64>(L, tw, st);
+  if (x == 8 && y == 64) return launch_tiles<S, 8, 64>(L, tw, st);
+  if (x == 16 && y == 64) return launch_tiles<S, 16, 64>(L, tw, st);
+  if (x == 8 && y == 128) return launch_tiles<S, 8, 128>(L, tw, st);
+  set_error("d2q9 tiles: unsupported tile shape %d x %d", x, y);
+  return HL_ERR_ARG;
+}
+
 template <class S> int run_phases(const d2::Launch& L, int n, int maxx, int maxy, bool any_solid, int phases,
-                                  cudaStream_t st) {
+                                  cudaStream_t st, const TileWork* tw = nullptr) {
   if ((phases & HL_PHASE_SEGMENTS) && any_solid) {
     d2::prologue_kernel<<<n, 256, 0, st>>>(L);
     HL_LAUNCH_CHECK("d2q9 precompute_transformed_segments");
   }
   if (phases & HL_PHASE_STREAM) {
-    dim3 grid((maxy + 31) / 32, (maxx + 7) / 8, n);
-    d2::stream_kernel<S><<<grid, 256, 0, st>>>(L);
-    HL_LAUNCH_CHECK("d2q9 stream_and_collide");
+    if (tw) {
+      const int rc = stream_tiles<S>(L, *tw, st);
+      if (rc != HL_OK) return rc;
+    } else {
+      dim3 grid((maxy + 31) / 32, (maxx + 7) / 8, n);
+      d2::stream_kernel<S><<<grid, 256, 0, st>>>(L);
+      HL_LAUNCH_CHECK("d2q9 stream_and_collide");
+    }
     if (any_solid) {
       d2::band_kernel<S><<<dim3(64, n), 256, 0, st>>>(L);
       HL_LAUNCH_CHECK("d2q9 cut-cell band");
@@ -584,12 +796,13 @@ template <class S> int run_phases(const d2::Launch& L, int n, int maxx, int maxy
   return HL_OK;
 }
 
-int dispatch(hl_dtype dt, const d2::Launch& L, int n, int maxx, int maxy, bool any_solid, int phases, cudaStream_t st) {
+int dispatch(hl_dtype dt, const d2::Launch& L, int n, int maxx, int maxy, bool any_solid, int phases, cudaStream_t st,
+             const TileWork* tw = nullptr) {
   switch (dt) {
-    case HL_F32: return run_phases<StoreF32>(L, n, maxx, maxy, any_solid, phases, st);
-    case HL_F64: return run_phases<StoreF64>(L, n, maxx, maxy, any_solid, phases, st);
-    case HL_F16: return run_phases<StoreF16>(L, n, maxx, maxy, any_solid, phases, st);
-    case HL_BF16: return run_phases<StoreBF16>(L, n, maxx, maxy, any_solid, phases, st);
+    case HL_F32: return run_phases<StoreF32>(L, n, maxx, maxy, any_solid, phases, st, tw);
+    case HL_F64: return run_phases<StoreF64>(L, n, maxx, maxy, any_solid, phases, st, tw);
+    case HL_F16: return run_phases<StoreF16>(L, n, maxx, maxy, any_solid, phases, st, tw);
+    case HL_BF16: return run_phases<StoreBF16>(L, n, maxx, maxy, any_solid, phases, st, tw);
   }
   set_error("d2q9: bad dtype");
   return HL_ERR_ARG;
@@ -628,6 +841,55 @@ extern "C" int hl_d2q9_step_batch(const void* desc_dev, int n_worlds, int parity
   L.many = static_cast<const d2::World*>(desc_dev);
   L.parity = parity;
   return dispatch(dtype, L, n_worlds, max_nx, max_ny, any_solid != 0, phases, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int hl_d2q9_tile_shapes(int32_t* out, int cap) {
+  for (int k = 0; k < N_TILE_SHAPES && k < cap && out; ++k) {
+    out[2 * k] = TILE_SHAPES[k][0];
+    out[2 * k + 1] = TILE_SHAPES[k][1];
+  }
+  return N_TILE_SHAPES;
+}
+
+extern "C" int hl_d2q9_tile_list(const int32_t* nx, const int32_t* ny, int n_worlds, int tile_x, int tile_y,
+                                 int32_t* out, size_t cap_tiles, size_t* n_tiles) {
+  HL_CHECK_ARG(nx != nullptr && ny != nullptr && n_tiles != nullptr && n_worlds > 0, "d2q9 tiles: bad arguments");
+  bool shape_ok = false;
+  for (int k = 0; k < N_TILE_SHAPES; ++k) shape_ok |= TILE_SHAPES[k][0] == tile_x && TILE_SHAPES[k][1] == tile_y;
+  HL_CHECK_ARG(shape_ok, "d2q9 tiles: unsupported tile shape %d x %d", tile_x, tile_y);
+  size_t count = 0;
+  for (int w = 0; w < n_worlds; ++w) {
+    HL_CHECK_ARG(nx[w] >= 3 && ny[w] >= 3 && nx[w] < (1 << 30) && ny[w] < (1 << 30), "d2q9 tiles: world %d is %d x %d",
+                 w, nx[w], ny[w]);
+    for (int x0 = 0; x0 < nx[w]; x0 += tile_x)
+      for (int y0 = 0; y0 < ny[w]; y0 += tile_y) {
+        if (out != nullptr && count < cap_tiles) {
+          out[4 * count] = w;
+          out[4 * count + 1] = x0;
+          out[4 * count + 2] = y0;
+          out[4 * count + 3] = 0;
+        }
+        ++count;
+      }
+  }
+  *n_tiles = count;
+  HL_CHECK_ARG(out == nullptr || count <= cap_tiles, "d2q9 tiles: %zu tiles do not fit in %zu", count, cap_tiles);
+  return HL_OK;
+}
+
+extern "C" int hl_d2q9_step_tiles(const void* desc_dev, int n_worlds, int parity, hl_dtype dtype,
+                                  const int32_t* tiles_dev, int n_tiles, int tile_x, int tile_y, int ctas,
+                                  int any_solid, int phases, hl_stream stream) {
+  HL_CHECK_ARG(desc_dev != nullptr && n_worlds > 0, "d2q9: bad batch arguments");
+  HL_CHECK_ARG(parity == 0 || parity == 1, "d2q9: parity must be 0 or 1");
+  HL_CHECK_ARG(n_tiles >= 0 && (n_tiles == 0 || tiles_dev != nullptr), "d2q9 tiles: tile list is NULL");
+  HL_CHECK_ARG(reinterpret_cast<uintptr_t>(tiles_dev) % 16 == 0, "d2q9 tiles: tile list must be 16-byte aligned");
+  HL_CHECK_ARG(ctas >= 1, "d2q9 tiles: grid must have at least one CTA");
+  d2::Launch L{};
+  L.many = static_cast<const d2::World*>(desc_dev);
+  L.parity = parity;
+  const TileWork tw{reinterpret_cast<const int4*>(tiles_dev), n_tiles, tile_x, tile_y, ctas};
+  return dispatch(dtype, L, n_worlds, 1, 1, any_solid != 0, phases, static_cast<cudaStream_t>(stream), &tw);
 }
 
 template <class S>

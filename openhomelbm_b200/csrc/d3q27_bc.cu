@@ -74,36 +74,19 @@ template <class S> __device__ __forceinline__ void store_cell(const BcArgs& a, l
 }
 
 // f_eq_home_3d (envs/lbm3d/lbm_func_3d.py:651-686): S of the unclamped second-order
-// equilibrium populations of (rho, u), from deviations f - w (S_aa = (sum - (rho-1)/3)/rho).
-// out = xx, yy, zz, xy, xz, yz.
-template <class R> __device__ void feq_s(R rho, R drho, R ux, R uy, R uz, R out[6]) {
-  const R usq = ux * ux + uy * uy + uz * uz;
-  R pxx = 0, pyy = 0, pzz = 0, pxy = 0, pxz = 0, pyz = 0;
-#pragma unroll
-  for (int cx = -1; cx <= 1; ++cx)
-#pragma unroll
-    for (int cy = -1; cy <= 1; ++cy)
-#pragma unroll
-      for (int cz = -1; cz <= 1; ++cz) {
-        const int nnz = (cx != 0) + (cy != 0) + (cz != 0);
-        const R w = nnz == 0 ? R(8.0 / 27.0) : nnz == 1 ? R(2.0 / 27.0) : nnz == 2 ? R(1.0 / 54.0) : R(1.0 / 216.0);
-        const R cu = R(cx) * ux + R(cy) * uy + R(cz) * uz;
-        const R f = w * (drho + rho * (R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq));
-        if (cx) pxx += f;
-        if (cy) pyy += f;
-        if (cz) pzz += f;
-        if (cx * cy) pxy += R(cx * cy) * f;
-        if (cx * cz) pxz += R(cx * cz) * f;
-        if (cy * cz) pyz += R(cy * cz) * f;
-      }
-  const R inv = R(1) / rho;
-  const R d3 = drho * R(1.0 / 3.0);
-  out[0] = (pxx - d3) * inv;
-  out[1] = (pyy - d3) * inv;
-  out[2] = (pzz - d3) * inv;
-  out[3] = pxy * inv;
-  out[4] = pxz * inv;
-  out[5] = pyz * inv;
+// equilibrium populations f_i = w_i (rho - 1 + rho (3 c.u + 4.5 (c.u)^2 - 1.5 u^2)), from
+// deviations f - w (S_aa = (P_aa - (rho-1)/3)/rho, S_ab = P_ab/rho). The D3Q27 weights give
+// sum w c_a c_b = delta_ab / 3, odd moments 0 and sum w c_a c_b c_c c_d = (delta_ab delta_cd +
+// delta_ac delta_bd + delta_ad delta_bc) / 9, so P_ab = (rho - 1) delta_ab / 3 + rho u_a u_b
+// and S_ab = u_a u_b exactly: computed in that closed form, not as the reference's 27-term
+// binary32 sums (which agree with it to their rounding). out = xx, yy, zz, xy, xz, yz.
+template <class R> __device__ __forceinline__ void feq_s(R ux, R uy, R uz, R out[6]) {
+  out[0] = ux * ux;
+  out[1] = uy * uy;
+  out[2] = uz * uz;
+  out[3] = ux * uy;
+  out[4] = ux * uz;
+  out[5] = uy * uz;
 }
 
 // apply_bc_core_3d (envs/lbm3d/lbm_func_3d.py:627-648): new state of boundary cell t from
@@ -122,8 +105,8 @@ template <class R> __device__ Mom3<R> bc_core(const BcArgs& a, int dr, const Mom
   r.rho = nb.rho;
   r.drho = nb.drho;
   R sc[6], sb[6];
-  feq_s<R>(r.rho, r.drho, r.ux, r.uy, r.uz, sc);
-  feq_s<R>(nb.rho, nb.drho, nb.ux, nb.uy, nb.uz, sb);
+  feq_s<R>(r.ux, r.uy, r.uz, sc);
+  feq_s<R>(nb.ux, nb.uy, nb.uz, sb);
   r.sxx = sc[0] - sb[0] + nb.sxx;
   r.syy = sc[1] - sb[1] + nb.syy;
   r.szz = sc[2] - sb[2] + nb.szz;

@@ -21,13 +21,16 @@
 // of any near solid has none (the rays are at most sqrt(3) long), and keeps the plain
 // kernel's result, which is the reference's arithmetic on plain links up to rounding. Each
 // remaining cell is computed by a whole warp, one lane per direction; its moments are warp
-// shuffle sums, and the loads are summed per block in shared memory and per solid in
-// binary64 global memory.
+// shuffle sums, and its loads are warp sums per solid hit, added per block in shared memory
+// and per solid in binary64 global memory.
 //
 // Ray-triangle test: Moller & Trumbore, "Fast, minimum storage ray-triangle intersection"
 // (1997), double-sided, closest hit with 0 <= t <= max_t = 2 (the reference's mesh query
-// bound, lbm_func_3d.py:308). Brute force over the solid's triangles: the band is small and
-// every thread of a warp reads the same triangle, so the loads broadcast.
+// bound, lbm_func_3d.py:308), over the triangles that the solid's bin lists for the cell (all
+// of them without bins), screened by the warp against the box the cell's links reach; every
+// lane (direction) then tests the survivors from shared memory. The screen only drops
+// triangles that no lane's exact test could report, so the hits are those of a test against
+// every triangle.
 
 #include <algorithm>
 #include <cmath>
@@ -211,12 +214,31 @@ template <class R> __device__ __forceinline__ R warp_sum(R v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
 
 // One near cell with a possible cut link, computed by a whole warp: lane i < 27 rebuilds the
 // population of direction i (a wall population with its momentum exchange if the link is
 // cut, the clamped neighbour population otherwise), the moments are warp sums, and lane 0
 // collides and stores the cell.
-constexpr int MAXC = 64;  // candidate triangles staged per batch, per warp
+constexpr int MAXC = 64;  // surviving candidate triangles staged per batch, per warp
+
+// Closest hit in [0, 1] over the staged triangles buf[0 .. m) for this lane's ray; updates
+// (cut, sid) when it is nearer than the current one (ties keep the lower solid).
+template <class R>
+__device__ __forceinline__ void test_staged(const float* buf, int m, bool active, V3<R> o, V3<R> d, int k, R& cut,
+                                            int& sid) {
+  R t;
+  if (active && m > 0 && ray_mesh<R>(buf, nullptr, m, o, d, R(2), &t)) {
+    if ((cut < R(0) || t < cut) && t >= R(0) && t <= R(1)) {
+      cut = t;
+      sid = k;
+    }
+  }
+}
 
 template <class S>
 __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, int z, unsigned mask) {
@@ -240,12 +262,17 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
   const bool active = i < 27 && xn >= 0 && xn < nx && yn >= 0 && yn < ny && zn >= 0 && zn < nz;
   // get_cutcell_multi_3d: the closest hit in [0, 1] over the solids near the cell. Which
   // solids and which candidate triangles depend on the cell only, so the loop is uniform
-  // across the warp: the warp stages each batch of candidates in shared memory together and
-  // every lane tests its own direction against it.
+  // across the warp. The warp screens the candidates 32 at a time (a lane per triangle)
+  // against the box that every link of the cell stays in, the cell's body-frame point
+  // +- the largest |component| of the lanes' ray directions, widened by 2e-3. That box holds
+  // each lane's segment box of ray_mesh's pre-test (widened by 1e-3), so a triangle outside
+  // it fails every lane's pre-test: dropping it changes no hit. The survivors are staged in
+  // shared memory and every lane tests its own direction against them.
   R cut = R(-1);
   int sid = -1;
   const V3<R> cell{R(x), R(y), R(z)};
   const V3<R> dir{-dx, -dy, -dz};
+  const unsigned lt_mask = (1u << i) - 1u;
   for (int k = 0; k < s.n_objects; ++k) {
     if (!in_mask(mask, k)) continue;  // no candidate triangles for this cell's rays
     const int t0 = s.tri_offset[k], ntri = s.tri_offset[k + 1] - t0;
@@ -258,27 +285,61 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
     const V3<R> ld = qrot(inv.qx, inv.qy, inv.qz, inv.qw, dir);
     const R sx = R(s.scale_sizes[3 * k]), sy = R(s.scale_sizes[3 * k + 1]), sz = R(s.scale_sizes[3 * k + 2]);
     const V3<R> los{lo.x / sx, lo.y / sy, lo.z / sz};
+    const V3<R> lds{ld.x / sx, ld.y / sy, ld.z / sz};
     const int32_t* list;
     int ncand;
     if (!candidates(s, k, ntri, los, sx, sy, sz, &list, &ncand)) continue;
+    const float rx = warp_max(i < 27 ? float(fabs(lds.x)) : 0.f) + 2e-3f;
+    const float ry = warp_max(i < 27 ? float(fabs(lds.y)) : 0.f) + 2e-3f;
+    const float rz = warp_max(i < 27 ? float(fabs(lds.z)) : 0.f) + 2e-3f;
+    const float bx0 = float(los.x) - rx, bx1 = float(los.x) + rx;
+    const float by0 = float(los.y) - ry, by1 = float(los.y) + ry;
+    const float bz0 = float(los.z) - rz, bz1 = float(los.z) + rz;
     const float* tk = s.tris + 9ll * t0;
-    for (int b0 = 0; b0 < ncand; b0 += MAXC) {
-      const int m = min(MAXC, ncand - b0);
-      __syncwarp();
-      for (int j = i; j < 9 * m; j += 32) {
-        const int q = b0 + j / 9;
-        buf[j] = tk[9 * (list ? list[q] : q) + j % 9];
-      }
-      __syncwarp();
-      R t;
-      if (active && ray_mesh<R>(buf, nullptr, m, los, {ld.x / sx, ld.y / sy, ld.z / sz}, R(2), &t)) {
-        if ((cut < R(0) || t < cut) && t >= R(0) && t <= R(1)) {
-          cut = t;
-          sid = k;
-        }
-      }
+    int nbuf = 0;
+    // software pipeline over the chunks: the vertices of chunk q + 1 and the list entries of
+    // chunk q + 2 are loaded while chunk q is screened
+    auto tri_of = [&](int q) { return list ? __ldg(list + q) : q; };
+    float vn[9];
+    if (i < ncand) {
+      const int t = tri_of(i);
+#pragma unroll
+      for (int j = 0; j < 9; ++j) vn[j] = __ldg(tk + 9 * t + j);
     }
+    int tri_n = 32 + i < ncand ? tri_of(32 + i) : 0;
+    for (int q0 = 0; q0 < ncand; q0 += 32) {
+      float v[9];
+#pragma unroll
+      for (int j = 0; j < 9; ++j) v[j] = vn[j];
+      const bool live = q0 + i < ncand;
+      if (q0 + 32 + i < ncand) {
+#pragma unroll
+        for (int j = 0; j < 9; ++j) vn[j] = __ldg(tk + 9 * tri_n + j);
+      }
+      if (q0 + 64 + i < ncand) tri_n = tri_of(q0 + 64 + i);
+      const bool keep = live && !(fmaxf(fmaxf(v[0], v[3]), v[6]) < bx0 || fminf(fminf(v[0], v[3]), v[6]) > bx1 ||
+                                  fmaxf(fmaxf(v[1], v[4]), v[7]) < by0 || fminf(fminf(v[1], v[4]), v[7]) > by1 ||
+                                  fmaxf(fmaxf(v[2], v[5]), v[8]) < bz0 || fminf(fminf(v[2], v[5]), v[8]) > bz1);
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      const int n = __popc(bal);
+      if (nbuf + n > MAXC) {  // uniform: flush the staged survivors first
+        __syncwarp();
+        test_staged<R>(buf, nbuf, active, los, lds, k, cut, sid);
+        nbuf = 0;
+        __syncwarp();
+      }
+      if (keep) {
+        float* dst = buf + 9 * (nbuf + __popc(bal & lt_mask));
+#pragma unroll
+        for (int j = 0; j < 9; ++j) dst[j] = v[j];
+      }
+      nbuf += n;
+    }
+    __syncwarp();
+    test_staged<R>(buf, nbuf, active, los, lds, k, cut, sid);
+    __syncwarp();
   }
+  double lf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // this link's momentum exchange and torque
   if (active) {
     const R wi = weight<R>(i);
     {
@@ -313,19 +374,31 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
         const R fx = cur_f * (ex - up.x) - pop * (dx - up.x);
         const R fy = cur_f * (ey - up.y) - pop * (dy - up.y);
         const R fz = cur_f * (ez - up.z) - pop * (dz - up.z);
-        double* L = acc + 6 * sid;
-        atomicAdd(&L[0], double(fx));
-        atomicAdd(&L[1], double(fy));
-        atomicAdd(&L[2], double(fz));
-        atomicAdd(&L[3], double(ry * fz - rz * fy));
-        atomicAdd(&L[4], double(rz * fx - rx * fz));
-        atomicAdd(&L[5], double(rx * fy - ry * fx));
+        lf[0] = double(fx);
+        lf[1] = double(fy);
+        lf[2] = double(fz);
+        lf[3] = double(ry * fz - rz * fy);
+        lf[4] = double(rz * fx - rx * fz);
+        lf[5] = double(rx * fy - ry * fx);
       } else {
         const Mom3<R> m = load_cell<S>(a, N, ((long long)xn * ny + yn) * nz + zn);
         pop = feq<R>(m.rho, m.ux, m.uy, m.uz, m.sxx, m.sxy, m.sxz, m.syy, m.syz, m.szz, dx, dy, dz, wi);
         if (pop < R(0)) pop = R(0);
       }
     }
+  }
+  // the loads of the cell's cut links, summed over the warp per solid hit (lanes of other
+  // solids add zero), then one shared-memory add per component
+  int pend = sid;  // >= 0 only on active lanes with a cut link
+  for (unsigned left = __ballot_sync(0xffffffffu, pend >= 0); left; left = __ballot_sync(0xffffffffu, pend >= 0)) {
+    const int target = __shfl_sync(0xffffffffu, pend, __ffs(left) - 1);
+    const bool mine = pend == target;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      const double v = warp_sum(mine ? lf[j] : 0.0);
+      if (i == 0) atomicAdd(&acc[6 * target + j], v);
+    }
+    if (mine) pend = -1;
   }
   // moments (lbm_func_3d.py:528-562) as warp sums: rho, the signed first moments and the
   // second moments (c_a^2 = |c_a|)
@@ -468,8 +541,20 @@ template <class S> __global__ void __launch_bounds__(BLOCK) classify_kernel(cons
   }
 }
 
+// solid_force / solid_torque <- binary32 copies of the binary64 sums of solid k (loaded
+// through L2: other blocks wrote them).
+__device__ __forceinline__ void loads_out(const hl_solids3d& s, int k) {
+  for (int j = 0; j < 3; ++j) {
+    if (s.force) s.force[3 * k + j] = float(__ldcg(&s.loads64[6 * k + j]));
+    if (s.torque) s.torque[3 * k + j] = float(__ldcg(&s.loads64[6 * k + 3 + j]));
+  }
+}
+
+// The block that finishes last (work[1] counts finished blocks; zeroed before the launch)
+// writes the binary32 loads.
 template <class S> __global__ void __launch_bounds__(BLOCK) process_kernel(const __grid_constant__ Args a) {
   __shared__ double acc[MAX_SOLIDS * 6];
+  __shared__ bool last;
   const hl_solids3d& s = a.s;
   const int n = s.n_objects;
   for (int k = threadIdx.x; k < 6 * n; k += blockDim.x) acc[k] = 0.0;
@@ -486,19 +571,22 @@ template <class S> __global__ void __launch_bounds__(BLOCK) process_kernel(const
     cut_cell<S>(a, acc, tri_buf[threadIdx.x >> 5], c / (ny * nz), (c / nz) % ny, c % nz, cm);
     __syncwarp();
   }
-  if (!__syncthreads_or(any)) return;
-  for (int k = threadIdx.x; k < 6 * n; k += blockDim.x)
-    if (acc[k] != 0.0) atomicAdd(&s.loads64[k], acc[k]);
+  if (__syncthreads_or(any)) {
+    for (int k = threadIdx.x; k < 6 * n; k += blockDim.x)
+      if (acc[k] != 0.0) atomicAdd(&s.loads64[k], acc[k]);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(reinterpret_cast<unsigned*>(s.work + 1), 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) loads_out(s, k);
 }
 
-// solid_force / solid_torque <- binary32 copies of the binary64 sums.
 __global__ void loads_out_kernel(hl_solids3d s) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= s.n_objects) return;
-  for (int j = 0; j < 3; ++j) {
-    if (s.force) s.force[3 * k + j] = float(s.loads64[6 * k + j]);
-    if (s.torque) s.torque[3 * k + j] = float(s.loads64[6 * k + 3 + j]);
-  }
+  if (k < s.n_objects) loads_out(s, k);
 }
 
 int num_sms_local() {
@@ -525,20 +613,22 @@ template <class S> int launch(const hl_world3d* w, double vis, const hl_solids3d
   const long long cells = (long long)a.box_side * a.box_side * a.box_side;
   const dim3 grid(unsigned((cells + BLOCK - 1) / BLOCK), unsigned(s->n_objects));
   if (s->work != nullptr) {
-    cudaError_t e = cudaMemsetAsync(s->work, 0, sizeof(int32_t), st);
+    // work[0]: listed cells, work[1]: finished process blocks
+    cudaError_t e = cudaMemsetAsync(s->work, 0, 2 * sizeof(int32_t), st);
     if (e != cudaSuccess) return cuda_status(e, "d3q27 solid links: zero work count");
     classify_kernel<S><<<grid, BLOCK, 0, st>>>(a);
     HL_LAUNCH_CHECK("d3q27 solid links (classify)");
     // four blocks per SM take the listed cells in turn (measured: smaller grids leave the
-    // densely listed bands of small domains to too few warps)
+    // densely listed bands of small domains to too few warps); the last block to finish
+    // writes the binary32 loads
     process_kernel<S><<<unsigned(4 * num_sms_local()), BLOCK, 0, st>>>(a);
     HL_LAUNCH_CHECK("d3q27 solid links (cut cells)");
   } else {
     band_kernel<S><<<grid, BLOCK, 0, st>>>(a);
     HL_LAUNCH_CHECK("d3q27 solid links (band)");
+    loads_out_kernel<<<(s->n_objects + 63) / 64, 64, 0, st>>>(*s);
+    HL_LAUNCH_CHECK("d3q27 solid links (loads)");
   }
-  loads_out_kernel<<<(s->n_objects + 63) / 64, 64, 0, st>>>(*s);
-  HL_LAUNCH_CHECK("d3q27 solid links (loads)");
   return HL_OK;
 }
 
@@ -576,5 +666,6 @@ extern "C" int hl_d3q27_solid_links(const hl_world3d* w, double vis_shear, const
 extern "C" size_t hl_d3q27_solid_links_work_ints(int n_objects, float max_bound_radius) {
   if (n_objects <= 0 || !(max_bound_radius >= 0.f) || max_bound_radius >= 512.f) return 0;
   const size_t side = size_t(d3s::box_side_of(max_bound_radius));
-  return 2 + 2 * size_t(n_objects) * side * side * side;  // count, pad, then (cell, solid mask) pairs
+  // count, finished-block counter, then (cell, solid mask) pairs
+  return 2 + 2 * size_t(n_objects) * side * side * side;
 }
