@@ -30,31 +30,58 @@ constexpr int MAX_SOLIDS = 64;
 // D2Q9 weight of direction i (lbm_core.py:127).
 template <class R> __device__ __forceinline__ R w2(int i) { return i == 0 ? R(4.0 / 9.0) : i < 5 ? R(1.0 / 9.0) : R(1.0 / 36.0); }
 
-// mlCalDistribution (envs/lbm/lbm_func.py:685-788): population i rebuilt from (rho, u, S)
-// with the third-order Hermite terms Axxy, Axyy, returned as the deviation f_i - w_i
-// (the reference's bracket minus one: w_i (rho - 1 + rho (bracket_i - 1))).
+// Explicitly rounded operations: the population arithmetic below is written with them, so
+// that every kernel using it rounds the same way whatever the surrounding code (the compiler
+// neither fuses nor splits them), and a population is the same number whichever kernel and
+// thread computes it.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// Third-order Hermite terms of mlCalDistribution (envs/lbm/lbm_func.py:695-696):
+// Axxy = Sxx uy + 2 Sxy ux - 2 ux^2 uy, Axyy = Syy ux + 2 Sxy uy - 2 ux uy^2.
 template <class R> __device__ __forceinline__ R third_xxy(const Mom2<R>& m) {
-  return m.sxx * m.uy + R(2) * m.sxy * m.ux - R(2) * m.ux * m.ux * m.uy;
+  const R u2 = mul_rn(mul_rn(R(2) * m.ux, m.ux), m.uy);
+  return fma_rn(m.sxx, m.uy, fma_rn(R(2) * m.sxy, m.ux, -u2));
 }
 template <class R> __device__ __forceinline__ R third_xyy(const Mom2<R>& m) {
-  return m.syy * m.ux + R(2) * m.sxy * m.uy - R(2) * m.ux * m.uy * m.uy;
+  const R u2 = mul_rn(mul_rn(R(2) * m.ux, m.uy), m.uy);
+  return fma_rn(m.syy, m.ux, fma_rn(R(2) * m.sxy, m.uy, -u2));
 }
-// The same with the third-order terms Axxy = third_xxy(m), Axyy = third_xyy(m) given.
+
+// mlCalDistribution (envs/lbm/lbm_func.py:685-788): population i rebuilt from (rho, u, S)
+// with the third-order Hermite terms Axxy, Axyy (given), returned as the deviation f_i - w_i
+// (the reference's bracket minus one: w_i (rho - 1 + rho (bracket_i - 1))). Products by 2 and
+// by powers of two are exact.
 template <class R> __device__ __forceinline__ R feq_dev_a(const Mom2<R>& m, R Axxy, R Axyy, int i) {
-  const R h = R(1.5);
+  const R h = R(1.5), s3 = R(3), q = R(4.5), n = R(9);
   R b;
   switch (i) {
-    case 0: b = -h * m.sxx - h * m.syy; break;
-    case 1: b = R(3) * m.ux + R(3) * m.sxx - h * m.syy - R(4.5) * Axyy; break;
-    case 2: b = -R(3) * m.ux + R(3) * m.sxx - h * m.syy + R(4.5) * Axyy; break;
-    case 3: b = R(3) * m.uy - h * m.sxx + R(3) * m.syy - R(4.5) * Axxy; break;
-    case 4: b = -R(3) * m.uy - h * m.sxx + R(3) * m.syy + R(4.5) * Axxy; break;
-    case 5: b = R(3) * (m.ux + m.uy) + R(3) * (m.sxx + m.syy + R(3) * m.sxy) + R(9) * (Axyy + Axxy); break;
-    case 6: b = -R(3) * m.ux + R(3) * m.uy + R(3) * (m.sxx + m.syy - R(3) * m.sxy) + R(9) * (Axxy - Axyy); break;
-    case 7: b = -R(3) * m.ux - R(3) * m.uy + R(3) * (m.sxx + m.syy + R(3) * m.sxy) - R(9) * (Axxy + Axyy); break;
-    default: b = R(3) * m.ux - R(3) * m.uy + R(3) * (m.sxx + m.syy - R(3) * m.sxy) - R(9) * (Axxy - Axyy); break;
+    case 0: b = fma_rn(-h, m.syy, mul_rn(-h, m.sxx)); break;
+    case 1: b = fma_rn(-q, Axyy, fma_rn(-h, m.syy, fma_rn(s3, m.sxx, mul_rn(s3, m.ux)))); break;
+    case 2: b = fma_rn(q, Axyy, fma_rn(-h, m.syy, fma_rn(s3, m.sxx, mul_rn(-s3, m.ux)))); break;
+    case 3: b = fma_rn(-q, Axxy, fma_rn(s3, m.syy, fma_rn(-h, m.sxx, mul_rn(s3, m.uy)))); break;
+    case 4: b = fma_rn(q, Axxy, fma_rn(s3, m.syy, fma_rn(-h, m.sxx, mul_rn(-s3, m.uy)))); break;
+    case 5:
+      b = fma_rn(n, add_rn(Axyy, Axxy), fma_rn(s3, fma_rn(s3, m.sxy, add_rn(m.sxx, m.syy)), mul_rn(s3, add_rn(m.ux, m.uy))));
+      break;
+    case 6:
+      b = fma_rn(n, add_rn(Axxy, -Axyy),
+                 fma_rn(s3, fma_rn(-s3, m.sxy, add_rn(m.sxx, m.syy)), fma_rn(s3, m.uy, mul_rn(-s3, m.ux))));
+      break;
+    case 7:
+      b = fma_rn(-n, add_rn(Axxy, Axyy),
+                 fma_rn(s3, fma_rn(s3, m.sxy, add_rn(m.sxx, m.syy)), fma_rn(-s3, m.uy, mul_rn(-s3, m.ux))));
+      break;
+    default:
+      b = fma_rn(-n, add_rn(Axxy, -Axyy),
+                 fma_rn(s3, fma_rn(-s3, m.sxy, add_rn(m.sxx, m.syy)), fma_rn(-s3, m.uy, mul_rn(s3, m.ux))));
+      break;
   }
-  return w2<R>(i) * (m.drho + m.rho * b);
+  return mul_rn(w2<R>(i), fma_rn(m.rho, b, m.drho));
 }
 template <class R> __device__ __forceinline__ R feq_dev(const Mom2<R>& m, int i) {
   return feq_dev_a<R>(m, third_xxy<R>(m), third_xyy<R>(m), i);
@@ -252,15 +279,53 @@ template <class S> __global__ void __launch_bounds__(256) stream_kernel(const __
 // ------------------------------------------------------------- 2b. stream over a tile work-list
 // The stream phase of batched worlds of different sizes as one persistent launch: the CTAs of
 // a fixed grid take the tiles of a work list in turn (tile t = {world, x0, y0, 0}, TX x TY
-// cells, clipped to the world). A CTA decodes the tile's moments and a one-cell halo into
-// shared memory (each moment plane read in coalesced rows along y), then computes every fluid
-// cell of the tile from there. The arithmetic is stream_kernel's (feq_dev_clamped, collide on
-// the same decoded moments), so the results are identical to it.
+// cells, clipped to the world). Source side: every source cell of the tile and its one-cell
+// halo is read once (coalesced rows along y) and decoded in registers; it rebuilds its
+// clamped populations and writes each one into the shared-memory mailbox of the destination
+// it streams to. A source outside a walled world writes -w_i (f = 0, stream_kernel's
+// out-of-range rule). After a barrier every fluid destination reads its nine populations,
+// collides and stores. Every population is stream_kernel's value (the same decode, the same
+// third-order terms, feq_dev_clamped and collide), so the results are identical to it.
 constexpr int TILE_THREADS = 256;
-constexpr int MOM2_WORDS = 9;  // rho, drho, ux, uy, sxx, syy, sxy, Axxy, Axyy
 
+// Mailbox of a TX x TY tile: [9][(TX + 2) x (TY + 2)] destination slots, padded by one cell
+// so that a source inside the tile writes all nine populations without checks (those that
+// land in the padding are never read).
 template <int TX, int TY, class R> constexpr size_t tile_smem_bytes() {
-  return size_t(TX + 2) * (TY + 2) * MOM2_WORDS * sizeof(R);
+  return size_t(9) * (TX + 2) * (TY + 2) * sizeof(R);
+}
+
+// Source cell at padded tile coordinates (hx, hy) (tile cell (hx - 1, hy - 1)): its
+// populations into the mailbox; CHECK: only those landing on a tile cell (halo sources).
+template <class S, int TX, int TY, bool CHECK>
+__device__ __forceinline__ void send_source(typename S::R* mb, int hx, int hy, int x0, int y0, int nx, int ny,
+                                            bool periodic, long long N, const typename S::T* __restrict__ cur,
+                                            const Scale& sc) {
+  using R = typename S::R;
+  constexpr int HY = TY + 2, HC = (TX + 2) * HY;
+  int gx = x0 - 1 + hx, gy = y0 - 1 + hy;
+  if (periodic) {
+    gx = wrap(gx, nx);
+    gy = wrap(gy, ny);
+  }
+  const bool in = gx >= 0 && gx < nx && gy >= 0 && gy < ny;
+  Mom2<R> m{};
+  R axxy = R(0), axyy = R(0);
+  if (in) {
+    const long long i = (long long)gx * ny + gy;
+    R raw[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) raw[k] = S::to_r(cur[k * N + i]);
+    m = decode2<S>(raw, sc);
+    axxy = third_xxy<R>(m);
+    axyy = third_xyy<R>(m);
+  }
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const int dx = hx + cx_of(i), dy = hy + cy_of(i);  // destination slot
+    if (CHECK && (dx < 1 || dx > TX || dy < 1 || dy > TY)) continue;
+    mb[i * HC + dx * HY + dy] = in ? feq_dev_clamped_a<R>(m, axxy, axyy, i) : -w2<R>(i);
+  }
 }
 
 template <class S, int TX, int TY>
@@ -268,9 +333,9 @@ __global__ void __launch_bounds__(TILE_THREADS) stream_tiles_kernel(const __grid
                                                                     const int4* __restrict__ tiles, int n_tiles) {
   using R = typename S::R;
   using T = typename S::T;
-  constexpr int HY = TY + 2, HC = (TX + 2) * HY;
+  constexpr int HY = TY + 2, HC = (TX + 2) * HY, NC = TX * TY, NH = 2 * HY + 2 * TX;
   extern __shared__ __align__(16) unsigned char tile_smem[];
-  R* sm = reinterpret_cast<R*>(tile_smem);  // [HC][9] decoded moments (and third-order terms)
+  R* mb = reinterpret_cast<R*>(tile_smem);
   for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
     const int4 tile = tiles[t];
     // the world's fields in registers: reads through the descriptor could not be kept across
@@ -287,61 +352,32 @@ __global__ void __launch_bounds__(TILE_THREADS) stream_tiles_kernel(const __grid
     const R omega = omega_of<R>(wd.vis_shear);
     const int x0 = tile.y, y0 = tile.z;
     const long long N = (long long)nx * ny;
-    __syncthreads();  // the previous tile's cells are done with the staged moments
-    for (int h = threadIdx.x; h < HC; h += TILE_THREADS) {
-      int gx = x0 - 1 + h / HY, gy = y0 - 1 + h % HY;
-      if (periodic) {
-        gx = wrap(gx, nx);
-        gy = wrap(gy, ny);
+    __syncthreads();  // the previous tile's destinations are done with the mailbox
+    for (int c = threadIdx.x; c < NC; c += TILE_THREADS)  // sources on the tile
+      send_source<S, TX, TY, false>(mb, 1 + c / TY, 1 + c % TY, x0, y0, nx, ny, periodic, N, cur, sc);
+    for (int k = threadIdx.x; k < NH; k += TILE_THREADS) {  // the ring of halo sources
+      int hx, hy;
+      if (k < 2 * HY) {
+        hx = k < HY ? 0 : TX + 1;
+        hy = k < HY ? k : k - HY;
+      } else {
+        const int j = k - 2 * HY;
+        hx = 1 + (j >> 1);
+        hy = (j & 1) ? TY + 1 : 0;
       }
-      if (gx >= 0 && gx < nx && gy >= 0 && gy < ny) {
-        const long long i = (long long)gx * ny + gy;
-        R raw[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) raw[k] = S::to_r(cur[k * N + i]);
-        const Mom2<R> m = decode2<S>(raw, sc);
-        R* d = sm + h * MOM2_WORDS;
-        d[0] = m.rho;
-        d[1] = m.drho;
-        d[2] = m.ux;
-        d[3] = m.uy;
-        d[4] = m.sxx;
-        d[5] = m.syy;
-        d[6] = m.sxy;
-        d[7] = third_xxy<R>(m);
-        d[8] = third_xyy<R>(m);
-      }
+      send_source<S, TX, TY, true>(mb, hx, hy, x0, y0, nx, ny, periodic, N, cur, sc);
     }
     __syncthreads();
-    for (int c = threadIdx.x; c < TX * TY; c += TILE_THREADS) {
+    for (int c = threadIdx.x; c < NC; c += TILE_THREADS) {
       const int lx = c / TY, ly = c % TY;
       const int x = x0 + lx, y = y0 + ly;
       if (x >= nx || y >= ny) continue;
       const long long ci = (long long)x * ny + y;
       if (flag ? flag[ci] != ML_FLUID : !periodic && !(x > 0 && x < nx - 1 && y > 0 && y < ny - 1)) continue;
+      const int slot = (lx + 1) * HY + ly + 1;
       R pop[9];
 #pragma unroll
-      for (int i = 0; i < 9; ++i) {
-        int xn = x - cx_of(i), yn = y - cy_of(i);
-        if (periodic) {
-          xn = wrap(xn, nx);
-          yn = wrap(yn, ny);
-        }
-        if (xn >= 0 && xn < nx && yn >= 0 && yn < ny) {
-          const R* q = sm + ((lx + 1 - cx_of(i)) * HY + (ly + 1 - cy_of(i))) * MOM2_WORDS;
-          Mom2<R> m;
-          m.rho = q[0];
-          m.drho = q[1];
-          m.ux = q[2];
-          m.uy = q[3];
-          m.sxx = q[4];
-          m.syy = q[5];
-          m.sxy = q[6];
-          pop[i] = feq_dev_clamped_a<R>(m, q[7], q[8], i);
-        } else {
-          pop[i] = -w2<R>(i);  // out of range: f = 0
-        }
-      }
+      for (int i = 0; i < 9; ++i) pop[i] = mb[i * HC + slot];
       const R Fx = fxp ? R(fxp[ci]) : R(0), Fy = fyp ? R(fyp[ci]) : R(0);
       R raw[6];
       encode2<S>(collide<R>(pop, Fx, Fy, omega), sc, raw);
