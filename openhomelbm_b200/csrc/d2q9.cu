@@ -180,7 +180,7 @@ template <class S> __device__ __forceinline__ void store2(const World& w, long l
   typename S::R raw[6];
   encode2<S>(v, w.sc, raw);
 #pragma unroll
-  for (int k = 0; k < 6; ++k) m[k * N + i] = S::from_r(raw[k]);
+  for (int k = 0; k < 6; ++k) m[k * N + i] = S::from_r(raw[k], unsigned(k * N + i));
 }
 
 __device__ __forceinline__ bool is_fluid(const World& w, int x, int y, long long i) {
@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(TILE_THREADS) stream_tiles_kernel(const __grid
       R raw[6];
       encode2<S>(collide<R>(pop, Fx, Fy, omega), sc, raw);
 #pragma unroll
-      for (int k = 0; k < 6; ++k) post[k * N + ci] = S::from_r(raw[k]);
+      for (int k = 0; k < 6; ++k) post[k * N + ci] = S::from_r(raw[k], unsigned(k * N + ci));
     }
   }
 }

@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(Tile<TY>::THREADS, 1) step_kernel(const StepAr
             R raw[10];
             encode3<S>(m, a.sc, raw);
 #pragma unroll
-            for (int k = 0; k < 10; ++k) post[k * N + c] = S::from_r(raw[k]);
+            for (int k = 0; k < 10; ++k) post[k * N + c] = S::from_r(raw[k], unsigned(k * N + c));
             if (DIAG) {
               mass += double(m.rho);
               bad += healthy<R>(m) ? 0 : 1;

@@ -70,7 +70,7 @@ template <class S> __device__ __forceinline__ void store_cell(const BcArgs& a, l
   typename S::R raw[10];
   encode3<S>(m, a.sc, raw);
 #pragma unroll
-  for (int k = 0; k < 10; ++k) p[k * a.N + i] = S::from_r(raw[k]);
+  for (int k = 0; k < 10; ++k) p[k * a.N + i] = S::from_r(raw[k], unsigned(k * a.N + i));
 }
 
 // f_eq_home_3d (envs/lbm3d/lbm_func_3d.py:651-686): S of the unclamped second-order

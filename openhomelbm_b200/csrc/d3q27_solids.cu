@@ -24,6 +24,13 @@
 // shuffle sums, and its loads are warp sums per solid hit, added per block in shared memory
 // and per solid in binary64 global memory.
 //
+// Geometry in binary32 in every storage build: the band membership, the rays in the body
+// frame and the hits are computed in binary32, as the reference's mesh query computes them, so
+// the binary64 build (the accuracy reference of the reduced storages) makes the same cut-link
+// decisions as the binary32 one and differs from it only by the fluid arithmetic. (Grazing
+// links flip between cut and uncut with the last bit of the ray geometry, which would make a
+// binary64 geometry a different boundary, not a more accurate one.)
+//
 // Ray-triangle test: Moller & Trumbore, "Fast, minimum storage ray-triangle intersection"
 // (1997), double-sided, closest hit with 0 <= t <= max_t = 2 (the reference's mesh query
 // bound, lbm_func_3d.py:308), over the triangles that the solid's bin lists for the cell (all
@@ -268,24 +275,26 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
   // each lane's segment box of ray_mesh's pre-test (widened by 1e-3), so a triangle outside
   // it fails every lane's pre-test: dropping it changes no hit. The survivors are staged in
   // shared memory and every lane tests its own direction against them.
-  R cut = R(-1);
+  float cut = -1.f;  // geometry in binary32 (see the file comment)
   int sid = -1;
   const V3<R> cell{R(x), R(y), R(z)};
   const V3<R> dir{-dx, -dy, -dz};
+  const V3<float> gcell{float(x), float(y), float(z)};
+  const V3<float> gdir{-float(ix), -float(iy), -float(iz)};
   const unsigned lt_mask = (1u << i) - 1u;
   for (int k = 0; k < s.n_objects; ++k) {
     if (!in_mask(mask, k)) continue;  // no candidate triangles for this cell's rays
     const int t0 = s.tri_offset[k], ntri = s.tri_offset[k + 1] - t0;
     if (ntri == 0) continue;
-    if (vlen(cell.x - R(s.position[3 * k]), cell.y - R(s.position[3 * k + 1]), cell.z - R(s.position[3 * k + 2])) >
-        R(s.bound_radius[k]) + R(2))
+    if (vlen(gcell.x - s.position[3 * k], gcell.y - s.position[3 * k + 1], gcell.z - s.position[3 * k + 2]) >
+        s.bound_radius[k] + 2.f)
       continue;
-    const Xf<R> inv = xinv(load_xf<R>(s.transforms + 7 * k));
-    const V3<R> lo = xpoint(inv, cell);
-    const V3<R> ld = qrot(inv.qx, inv.qy, inv.qz, inv.qw, dir);
-    const R sx = R(s.scale_sizes[3 * k]), sy = R(s.scale_sizes[3 * k + 1]), sz = R(s.scale_sizes[3 * k + 2]);
-    const V3<R> los{lo.x / sx, lo.y / sy, lo.z / sz};
-    const V3<R> lds{ld.x / sx, ld.y / sy, ld.z / sz};
+    const Xf<float> inv = xinv(load_xf<float>(s.transforms + 7 * k));
+    const V3<float> lo = xpoint(inv, gcell);
+    const V3<float> ld = qrot(inv.qx, inv.qy, inv.qz, inv.qw, gdir);
+    const float sx = s.scale_sizes[3 * k], sy = s.scale_sizes[3 * k + 1], sz = s.scale_sizes[3 * k + 2];
+    const V3<float> los{lo.x / sx, lo.y / sy, lo.z / sz};
+    const V3<float> lds{ld.x / sx, ld.y / sy, ld.z / sz};
     const int32_t* list;
     int ncand;
     if (!candidates(s, k, ntri, los, sx, sy, sz, &list, &ncand)) continue;
@@ -324,7 +333,7 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
       const int n = __popc(bal);
       if (nbuf + n > MAXC) {  // uniform: flush the staged survivors first
         __syncwarp();
-        test_staged<R>(buf, nbuf, active, los, lds, k, cut, sid);
+        test_staged<float>(buf, nbuf, active, los, lds, k, cut, sid);
         nbuf = 0;
         __syncwarp();
       }
@@ -336,7 +345,7 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
       nbuf += n;
     }
     __syncwarp();
-    test_staged<R>(buf, nbuf, active, los, lds, k, cut, sid);
+    test_staged<float>(buf, nbuf, active, los, lds, k, cut, sid);
     __syncwarp();
   }
   double lf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // this link's momentum exchange and torque
@@ -346,7 +355,8 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
       if (sid >= 0) {
         const Xf<R> tc = load_xf<R>(s.transforms + 7 * sid);
         const Xf<R> tl = load_xf<R>(s.transforms_last + 7 * sid);
-        const V3<R> hit{cell.x + dir.x * cut, cell.y + dir.y * cut, cell.z + dir.z * cut};
+        const R rc = R(cut);
+        const V3<R> hit{cell.x + dir.x * rc, cell.y + dir.y * rc, cell.z + dir.z * rc};
         const V3<R> hl = xpoint(xinv(tc), hit);
         V3<R> up;
         const R spx = R(s.position[3 * sid]), spy = R(s.position[3 * sid + 1]), spz = R(s.position[3 * sid + 2]);
@@ -448,7 +458,7 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
   encode3<S>(m, a.sc, raw);
   T* post = static_cast<T*>(a.w.post);
 #pragma unroll
-  for (int k = 0; k < 10; ++k) post[k * N + c] = S::from_r(raw[k]);
+  for (int k = 0; k < 10; ++k) post[k * N + c] = S::from_r(raw[k], unsigned(k * N + c));
 }
 
 template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __grid_constant__ Args a) {
@@ -480,7 +490,8 @@ template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __
     const long long c = ((long long)x * ny + y) * nz + z;
     const bool fluid = inside && (a.w.flag == nullptr || a.w.flag[c] == ML_FLUID) &&
                        (a.w.flag != nullptr || a.w.periodic || (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1));
-    if (fluid && first_near<R>(s, R(x), R(y), R(z)) == k0) solids = cut_mask<R>(s, V3<R>{R(x), R(y), R(z)});
+    if (fluid && first_near<float>(s, float(x), float(y), float(z)) == k0)
+      solids = cut_mask<float>(s, V3<float>{float(x), float(y), float(z)});
     flagged = solids != 0u;
   }
   // 2. the warp computes its flagged cells one after another, a lane per direction
@@ -525,7 +536,8 @@ template <class S> __global__ void __launch_bounds__(BLOCK) classify_kernel(cons
     c = (x * ny + y) * nz + z;
     const bool fluid = inside && (a.w.flag == nullptr || a.w.flag[c] == ML_FLUID) &&
                        (a.w.flag != nullptr || a.w.periodic || (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1));
-    if (fluid && first_near<R>(s, R(x), R(y), R(z)) == k0) solids = cut_mask<R>(s, V3<R>{R(x), R(y), R(z)});
+    if (fluid && first_near<float>(s, float(x), float(y), float(z)) == k0)
+      solids = cut_mask<float>(s, V3<float>{float(x), float(y), float(z)});
     flagged = solids != 0u;
   }
   const unsigned mask = __ballot_sync(0xffffffffu, flagged);

@@ -489,11 +489,11 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
           encode_pair<S>(m, a.sc, raw);
           if (f0) {
 #pragma unroll
-            for (int k = 0; k < 10; ++k) post[k * N + c0] = S::from_r(raw[k].x());
+            for (int k = 0; k < 10; ++k) post[k * N + c0] = S::from_r(raw[k].x(), unsigned(k * N + c0));
           }
           if (f1) {
 #pragma unroll
-            for (int k = 0; k < 10; ++k) post[k * N + c1] = S::from_r(raw[k].y());
+            for (int k = 0; k < 10; ++k) post[k * N + c1] = S::from_r(raw[k].y(), unsigned(k * N + c1));
           }
           if (DIAG) {
             const P2 s = m.ux + m.uy + m.uz + m.sxx + m.syy + m.szz + m.sxy + m.sxz + m.syz;
