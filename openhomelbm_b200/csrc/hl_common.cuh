@@ -67,40 +67,36 @@ inline Scale make_scale(const hl_storage& st) {
 // goes to the upper one with probability equal to its distance from the lower one, in units
 // of their spacing (unbiased in expectation). Round-to-nearest stores of a slowly varying
 // field round the same way step after step and its error drifts; stochastic rounding makes
-// the per-step errors independent. The random bits are an integer hash (the "lowbias32" mixer
-// of C. Wellons' hash-prospector, public domain) of the value's own bit pattern and a salt
-// (the element's index in its buffer), so a store is a deterministic function of the value and
-// its place: a field gives the same result in every run, alone or batched, while equal values
-// in different cells round independently. The hash bits are uniform and unrelated to the
-// dropped low bits, which is what unbiasedness needs.
-__device__ __forceinline__ unsigned dither_bits(unsigned x) {
-  x ^= x >> 16;
-  x *= 0x7feb352du;
-  x ^= x >> 15;
-  x *= 0x846ca68bu;
-  x ^= x >> 16;
-  return x;
+// the per-step errors independent. The random bits are the top bits of a multiplicative hash
+// (Knuth's multiplicative hashing, golden-ratio and MurmurHash3-finaliser constants) of the
+// value's own bit pattern and a salt (the element's index in its buffer): a store is a
+// deterministic function of the value and its place, so a field gives the same result in
+// every run, alone or batched, while equal values in different cells round independently.
+// The top bits of the product depend on every input bit, the dropped low bits included, and
+// are uniform over the values and places a field holds, which is what unbiasedness needs.
+__device__ __forceinline__ unsigned dither_bits(unsigned b, unsigned salt) {
+  return (b ^ (salt * 0x9e3779b9u)) * 0x85ebca6bu;
 }
 // binary32 -> binary16, stochastic. Normal range: add 13 random bits below the binary16 unit
 // of the last place to the magnitude and truncate. Below the smallest normal (2^-14) the
 // spacing is the fixed 2^-24: floor(v 2^24 + U), U uniform in [0, 1), then exact.
 __device__ __forceinline__ __half half_sr(float v, unsigned salt) {
   const unsigned b = __float_as_uint(v);
-  const unsigned h = dither_bits(b ^ (salt * 0x9e3779b9u));
-  if ((b & 0x7f800000u) == 0x7f800000u) return __float2half_rn(v);  // inf, nan
+  const unsigned h = dither_bits(b, salt);
   if (fabsf(v) < 6.103515625e-05f) {
     const float q = v * 16777216.f;                        // exact
     const float u = float(h >> 8) * (1.0f / 16777216.f);   // [0, 1)
     return __float2half_rn(floorf(q + u) * 5.9604644775390625e-08f);
   }
-  return __float2half_rz(__uint_as_float(b + (h & 0x1fffu)));
+  const unsigned r = (b & 0x7f800000u) == 0x7f800000u ? 0u : h >> 19;  // inf, nan unchanged
+  return __float2half_rz(__uint_as_float(b + r));
 }
 // binary32 -> bfloat16, stochastic: 16 random bits below the bfloat16 unit of the last place
 // (same exponent range as binary32, so no subnormal case short of binary32's own).
 __device__ __forceinline__ __nv_bfloat16 bf16_sr(float v, unsigned salt) {
   const unsigned b = __float_as_uint(v);
-  if ((b & 0x7f800000u) == 0x7f800000u) return __float2bfloat16_rn(v);  // inf, nan
-  return __float2bfloat16_rz(__uint_as_float(b + (dither_bits(b ^ (salt * 0x9e3779b9u)) & 0xffffu)));
+  const unsigned r = (b & 0x7f800000u) == 0x7f800000u ? 0u : dither_bits(b, salt) >> 16;  // inf, nan unchanged
+  return __float2bfloat16_rz(__uint_as_float(b + r));
 }
 
 struct StoreF32 {
