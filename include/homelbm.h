@@ -359,6 +359,41 @@ HL_API int hl_d2q9_init_uniform(int nx, int ny, hl_storage storage, void* m_a, v
 /* Replaces InitBoundary (envs/lbm/lbm_func.py:17-23). */
 HL_API int hl_d2q9_init_boundary(int nx, int ny, int32_t* flag, hl_stream stream);
 
+/* Field diagnostics: headless images of a world's current moments (cur), the arithmetic of the
+ * reference's display kernels, into a caller-owned binary32 device buffer (no GL texture).
+ *
+ * hl_d2q9_image, out [nx][ny] (kind 1: [nx][ny][3]):
+ *   kind 0  |u|                                   get_u_img (envs/lbm/lbm_func.py:163-166)
+ *   kind 1  (|u|, ux, uy) / param mapped to [0, 1]  get_velocity_rgb (169-193), param = max_velocity
+ *   kind 2  dv/dx - du/dy, one-sided on the border  get_vorticity_img (196-233); with solids,
+ *           pixels inside a polygon or within `thickness` of one are 1000
+ *           (get_vorticity_with_solid_img, 236-319)
+ *   kind 3  1 inside or within `thickness` of a polygon, else 0  get_solid_boundary_img (804-866)
+ * grid_length <= 0 selects 1/nx (HomeFlow.grid_length). solids (kinds 2, 3) use line_tf,
+ * line_num, position, scale and max_radius; NULL or no objects: no overlay.
+ *
+ * hl_d3q27_image (envs/lbm3d/lbm_func_3d.py:753-1313), out [na][nb] over the two axes other than
+ * `axis` in increasing order (axis 2: (x, y); axis 0: (y, z); axis 1: (x, z)):
+ *   mode 0, slice at coordinate `index` along `axis`:
+ *     kind 0  |u|                               get_u_img_xy_3d / get_u_img_yz_3d
+ *     kind 1  the vorticity component along `axis` (z: dv/dx - du/dy, x: dw/dy - dv/dz,
+ *             y: du/dz - dw/dx)               get_vorticity_xy_3d / _yz_3d; with solids, voxels
+ *             flagged ML_SOLID, inside a mesh or within `thickness` of it are 1000 (_with_solid_3d)
+ *   mode 1, projection seen from beyond the high end of `axis`, looking down it:
+ *     kind 0  max |u| over the column, walls skipped  get_u_projection_max_topdown_3d,
+ *             get_u_projection_side_3d (axis 0), get_u_projection_front_3d (axis 1)
+ *     kind 1  |u| of the first moving cell from the viewer  get_u_projection_topdown_3d
+ *     kind 2  the vorticity component along `axis` of largest magnitude, sign kept
+ *             get_vorticity_projection_topdown_3d / _side_3d / _front_3d
+ *     with solids, a column whose ray from the viewer hits a mesh is 1000
+ *     (any_mesh_hit_along_ray_3d, 320-362).
+ * solids uses tri_offset, tris, transforms and scale_sizes. Calls are stream-ordered, allocate
+ * nothing and can be captured in a CUDA graph. */
+HL_API int hl_d2q9_image(const hl_world2d* w, int kind, float param, float grid_length, const hl_solids2d* solids,
+                         float thickness, float* out, hl_stream stream);
+HL_API int hl_d3q27_image(const hl_world3d* w, int mode, int axis, int index, int kind, float grid_length,
+                          const hl_solids3d* solids, float thickness, float* out, hl_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -105,6 +105,10 @@ _SIGS = {
                       c_void_p], c_int),
     "hl_d2q9_step_batch": ([c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p], c_int),
     "hl_d2q9_tile_shapes": ([c_void_p, c_int], c_int),
+    "hl_d2q9_image": ([POINTER(hl_world2d), c_int, c_float, c_float, POINTER(hl_solids2d), c_float, c_void_p, c_void_p],
+                      c_int),
+    "hl_d3q27_image": ([POINTER(hl_world3d), c_int, c_int, c_int, c_int, c_float, POINTER(hl_solids3d), c_float, c_void_p,
+                        c_void_p], c_int),
     "hl_d2q9_tile_list": ([c_void_p, c_void_p, c_int, c_int, c_int, c_void_p, c_size_t, POINTER(c_size_t)], c_int),
     "hl_d2q9_step_tiles": ([c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_int, c_int, c_int, c_int, c_int,
                             c_void_p], c_int),

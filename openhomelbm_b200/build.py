@@ -21,8 +21,9 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-r
               "-Xcompiler", "-fvisibility=hidden"]
 # Per-file flags. The immersed-solid band decides hit or miss per link from binary32 ray
 # geometry; a link that grazes a mesh edge flips with the last bit, so that file rounds every
-# multiply and add separately, as the reference's binary32 arithmetic does.
-FILE_FLAGS = {"d3q27_solids.cu": ["-fmad=false"]}
+# multiply and add separately, as the reference's binary32 arithmetic does. The diagnostics'
+# solid overlays make the same kind of decisions (inside, within a thickness, ray hits).
+FILE_FLAGS = {"d3q27_solids.cu": ["-fmad=false"], "diagnostics.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:

@@ -33,6 +33,7 @@ extern int g_tune_d3_stages;  // hl_set_tuning("d3q27_stages")
 
 // ----------------------------------------------------------------------------- lattice
 constexpr int ML_FLUID = 0;
+constexpr int ML_SOLID = 1;
 constexpr int ML_WALL = 2;
 constexpr float CS2 = 1.0f / 3.0f;
 

@@ -81,11 +81,13 @@ class LBM_Solver3D:
         self._graphs = {}
         self._graph_key = None
         self.flows = []
-        for _ in range(self.nworld):
+        for k in range(self.nworld):
             f = HomeFlow3D()
             f.Initialize(nx, ny, nz, n_objects=solid_num, device=self.device, storage=storage,
                          u_scale=u_scale, s_scale=s_scale, periodic=periodic, with_flag=with_flag,
                          with_force=with_force)
+            # the solver holds the meshes; the field diagnostics find them from the world
+            f.solver, f.world_index = self, k
             self.flows.append(f)
         stream = _lib.stream_ptr()
         L = _lib.lib()
