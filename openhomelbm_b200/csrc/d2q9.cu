@@ -428,13 +428,16 @@ __device__ Cut get_cutcell(const World& w, float x, float y, float dx, float dy)
 // (solid, segment) order, holding every segment of a near solid that can cross a link of the
 // cell. The per-segment arithmetic and the tie rule (first nearest wins) are get_cutcell's, so
 // the result is the same.
-__device__ Cut get_cutcell_list(const World& w, const int* cand, int nc, float x, float y, float dx, float dy) {
+// tf_all / nseg_all: the world's transformed segments [n][max_segments][2] and segment counts
+// (shared-memory copies or the world's own arrays).
+__device__ Cut get_cutcell_list(const float* tf_all, const int* nseg_all, int max_segments, const int* cand, int nc,
+                                float x, float y, float dx, float dy) {
   Cut r{-1.f, -1.f, -1, -1};
   const float ax = x - dx, ay = y - dy, bx = x, by = y;
   for (int k = 0; k < nc; ++k) {
     const int s = cand[k] >> 16, n = cand[k] & 0xffff;
-    const int nseg = w.line_num[s];
-    const float* tf = w.tf + size_t(s) * w.max_segments * 2;
+    const int nseg = nseg_all[s];
+    const float* tf = tf_all + size_t(s) * max_segments * 2;
     const int n1 = n + 1 == nseg ? 0 : n + 1;
     const float cx = tf[2 * n], cy = tf[2 * n + 1], ex = tf[2 * n1], ey = tf[2 * n1 + 1];
     const float abc = (ax - cx) * (by - cy) - (ay - cy) * (bx - cx);
@@ -455,22 +458,42 @@ __device__ Cut get_cutcell_list(const World& w, const int* cand, int nc, float x
 }
 
 constexpr int MAX_CAND = 24;  // candidate segments kept per cell; more: the full scan
+constexpr int BAND_TF_FLOATS = 4096;  // transformed segment coordinates staged per block
 
 template <class S> __global__ void __launch_bounds__(256) band_kernel(const __grid_constant__ Launch L) {
   using R = typename S::R;
   using T = typename S::T;
   const World& w = world_of(L, blockIdx.y);
   if (w.n_objects == 0 || w.box == nullptr) return;  // a world of the batch without solids
+  const int x0 = w.box[0], x1 = w.box[1], y0 = w.box[2], y1 = w.box[3];
+  // (block-uniform) a block past the end of the band has no cell
+  if (x0 > x1 || y0 > y1 || (long long)blockIdx.x * blockDim.x >= (long long)(x1 - x0 + 1) * (y1 - y0 + 1)) return;
   __shared__ double acc[MAX_SOLIDS * 3];
   __shared__ int touched;
+  // the world's per-solid band radii and segments, read by every cell's screening and ray
+  // tests: staged in shared memory (the segments when they fit)
+  __shared__ float s_tf[BAND_TF_FLOATS];
+  __shared__ float s_px[MAX_SOLIDS], s_py[MAX_SOLIDS], s_r2[MAX_SOLIDS];
+  __shared__ int s_nseg[MAX_SOLIDS];
   const int nsol = min(w.n_objects, MAX_SOLIDS);
+  const int n_tf = w.n_objects * w.max_segments * 2;
+  const bool staged = w.n_objects <= MAX_SOLIDS && n_tf <= BAND_TF_FLOATS;
   for (int k = threadIdx.x; k < nsol * 3; k += blockDim.x) acc[k] = 0.0;
+  for (int s = threadIdx.x; s < nsol; s += blockDim.x) {
+    const float scale = w.scale[s] * float(w.nx);
+    s_px[s] = w.position[2 * s];
+    s_py[s] = w.position[2 * s + 1];
+    s_r2[s] = w.max_radius[s] * scale * scale;
+    s_nseg[s] = w.line_num[s];
+  }
+  if (staged)
+    for (int k = threadIdx.x; k < n_tf; k += blockDim.x) s_tf[k] = w.tf[k];
   if (threadIdx.x == 0) touched = 0;
   __syncthreads();
-  const int x0 = w.box[0], x1 = w.box[1], y0 = w.box[2], y1 = w.box[3];
+  const float* tfb = staged ? s_tf : w.tf;
   const long long N = (long long)w.nx * w.ny;
   const T* cur = static_cast<const T*>(cur_of(L, w));
-  if (x0 <= x1 && y0 <= y1) {
+  {
     const int bw = y1 - y0 + 1;
     const long long area = (long long)(x1 - x0 + 1) * bw;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < area;
@@ -486,13 +509,12 @@ template <class S> __global__ void __launch_bounds__(256) band_kernel(const __gr
       int nc = 0;
       bool overflow = false;
       const float fxc = float(x), fyc = float(y);
-      for (int s = 0; s < w.n_objects; ++s) {
-        const int nseg = w.line_num[s];
+      for (int s = 0; s < nsol; ++s) {
+        const int nseg = s_nseg[s];
         if (nseg <= 0) continue;
-        const float px = fxc - w.position[2 * s], py = fyc - w.position[2 * s + 1];
-        const float scale = w.scale[s] * float(w.nx);
-        if (px * px + py * py > w.max_radius[s] * scale * scale) continue;
-        const float* tf = w.tf + size_t(s) * w.max_segments * 2;
+        const float px = fxc - s_px[s], py = fyc - s_py[s];
+        if (px * px + py * py > s_r2[s]) continue;
+        const float* tf = tfb + size_t(s) * w.max_segments * 2;
         for (int n = 0; n < nseg; ++n) {
           const int n1 = n + 1 == nseg ? 0 : n + 1;
           const float cx = tf[2 * n], cy = tf[2 * n + 1], ex = tf[2 * n1], ey = tf[2 * n1 + 1];
@@ -519,7 +541,8 @@ template <class S> __global__ void __launch_bounds__(256) band_kernel(const __gr
         pop[i] = -w2<R>(i);
         if (!(xn >= 0 && xn < w.nx && yn >= 0 && yn < w.ny)) continue;
         const Cut cc = overflow ? get_cutcell(w, fxc, fyc, float(cx_of(i)), float(cy_of(i)))
-                                : get_cutcell_list(w, cand, nc, fxc, fyc, float(cx_of(i)), float(cy_of(i)));
+                                : get_cutcell_list(tfb, s_nseg, w.max_segments, cand, nc, fxc, fyc, float(cx_of(i)),
+                                                   float(cy_of(i)));
         if (cc.t >= 0.f && cc.solid >= 0) {
           any_cut = true;
           const int s = cc.solid, nseg = w.line_num[s];
