@@ -146,21 +146,24 @@ class LBM_Solver:
     def create_solid_from_mujoco(self, solid_id: int, model: Any, data: Any, body_or_geom_name: str,
                                  lbm_position: Optional[Tuple[float, float]] = None, lbm_scale: Optional[float] = 0.3,
                                  n_samples: int = 20, is_body: bool = True, **kwargs: Any) -> Dict[str, Any]:
-        """Project a MuJoCo body into every world (lbm_solver.py:143-209).
+        """Project a MuJoCo body (or geom) into every world (lbm_solver.py:143-209).
 
-        The projection itself (envs/lbm/mujoco_to_lbm.py) is host-side geometry preparation that
-        this package does not re-implement; pass a callable ``project(model, data, name,
-        n_samples, is_body)`` returning {'vertices', 'angle', 'position'} as ``project=``.
+        The outline comes from ``openhomelbm_b200.geometry.extract_lbm_polygon_from_mujoco``
+        (convex hull, centred), or from a callable ``project(model, data, name, n_samples,
+        is_body)`` returning {'vertices', 'angle', 'position'} passed as ``project=``. Returns
+        the projection, as the reference does.
         """
         project = kwargs.pop("project", None)
         if project is None:
-            raise NotImplementedError(
-                "MuJoCo geometry projection is outside this package; pass project=... or use "
-                "create_solid_from_polygon")
-        info = project(model, data, body_or_geom_name, n_samples, is_body)
-        out = self.create_solid_from_polygon(solid_id, info["vertices"], lbm_position, lbm_scale, info["angle"],
-                                             mujoco_origin=info.get("position"), **kwargs)
-        return {**info, **out}
+            from ..geometry import extract_lbm_polygon_from_mujoco
+
+            info = extract_lbm_polygon_from_mujoco(model, data, body_or_geom_name, n_samples=n_samples,
+                                                   use_convex_hull=True, normalize=True, is_body=is_body)
+        else:
+            info = project(model, data, body_or_geom_name, n_samples, is_body)
+        self.create_solid_from_polygon(solid_id, info["vertices"], lbm_position, lbm_scale, info["angle"],
+                                       mujoco_origin=info.get("position"), **kwargs)
+        return info
 
     def finalize_mappings(self, solid_ids: Sequence[int]) -> None:
         """Coordinate-mapping arrays for batch coupling (lbm_solver.py:211-244)."""

@@ -169,3 +169,28 @@ def test_d2q9_uniform_init_matches_reference_fixture():
     # the reference forms S from sums of populations of size ~1/3: two ulps of 1/3
     for buf, ref in ((f.cur, g["moments2"]), (f.post, g["post2"])):
         np.testing.assert_allclose(buf.cpu().numpy(), ref, rtol=0, atol=6e-8)
+
+
+def test_create_solid_from_mujoco_uses_the_geometry_projection():
+    """LBM_Solver.create_solid_from_mujoco on a stand-in MuJoCo model (MuJoCo's field names):
+    the solid equals create_solid_from_polygon with the projection of
+    openhomelbm_b200.geometry.extract_lbm_polygon_from_mujoco, and the MuJoCo mapping records
+    the body's xy position."""
+    from test_geometry import _fake_model
+
+    from openhomelbm_b200.geometry import extract_lbm_polygon_from_mujoco
+    from openhomelbm_b200.lbm import LBM_Solver
+
+    model, data, _ = _fake_model()
+    a = LBM_Solver(64, 48, solid_num=1, use_graph=False)
+    info = a.create_solid_from_mujoco(0, model, data, "b", lbm_position=(30.0, 24.0), lbm_scale=0.2)
+    ref = extract_lbm_polygon_from_mujoco(model, data, "b")
+    np.testing.assert_array_equal(info["vertices"], ref["vertices"])
+    b = LBM_Solver(64, 48, solid_num=1, use_graph=False)
+    b.create_solid_from_polygon(0, ref["vertices"], (30.0, 24.0), 0.2, ref["angle"], mujoco_origin=ref["position"])
+    fa, fb = a.flows[0], b.flows[0]
+    for name in ("solid_line", "solid_line_num", "solid_position", "solid_angle", "solid_scale", "solid_max_radius"):
+        assert torch.equal(getattr(fa, name), getattr(fb, name)), name
+    assert int(fa.solid_line_num[0]) == len(ref["vertices"]) > 3
+    np.testing.assert_allclose(a.mujoco_mappings[0]["mujoco_origin"], [3.0, 3.0])
+    assert a.mujoco_mappings[0]["scale"] == pytest.approx(0.2 * 64)

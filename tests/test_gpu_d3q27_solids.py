@@ -174,3 +174,46 @@ def test_solid_links_rejects_bad_arguments():
     assert rc == _lib.HL_ERR_ARG
     with pytest.raises(ValueError):
         s.create_solid_from_mesh(2, _icosahedron())
+
+
+def test_mjcf_body_mesh_vs_oracle(tmp_path):
+    """A body meshed from MJCF by openhomelbm_b200.geometry (a capsule given by fromto and a
+    box, merged into one closed triangle mesh) as the solid of a walled 48x40x40 box: 4 steps
+    against the oracle, binary32 storage."""
+    from openhomelbm_b200 import geometry
+    from openhomelbm_b200.lbm3d import LBM_Solver3D
+
+    p = tmp_path / "fish.xml"
+    p.write_text('<mujoco model="fish"><worldbody><body name="torso" pos="0 0 0">'
+                 '<geom type="capsule" fromto="-0.3 0 0 0.3 0 0" size="0.12"/>'
+                 '<geom type="box" size="0.1 0.05 0.2" pos="0.3 0 0"/></body></worldbody></mujoco>')
+    mesh = geometry.parse_mjcf_to_meshes(str(p))["torso"]
+    nx, ny, nz = 48, 40, 40
+    u = (0.03, 0.0, 0.01)
+    s = LBM_Solver3D(nx, ny, nz, solid_num=1)
+    f = s.flows[0]
+    f.vis_shear = 0.02
+    f.bc_type = [0, 1, 1, 1, 1, 1]
+    f.bc_value = np.array([u] + [(0, 0, 0)] * 5, np.float32)
+    s.set_uniform_flow(*u)
+    s.create_solid_from_mesh(0, mesh, lbm_position=(20.3, 19.6, 20.4), lbm_scale=20.0 / nx,
+                                    init_quaternion=tuple(_quat((0, 1, 1), 0.4)))
+    assert abs(float(f.solid_bound_radius[0]) - 9.0) < 1e-4  # box corner (0.4, 0.05, 0.2) x 20
+    flag = orc.border_flags_3d(nx, ny, nz)
+    m0 = f.decoded().double().cpu().numpy()
+    m32, p32 = m0.astype(np.float32), m0.astype(np.float32)
+    m64, p64 = m0.copy(), m0.copy()
+    for step in range(4):
+        solids = _solids_from(s)
+        s.step()
+        new, l32 = orc.step_3d(m32, p32, vis_shear=np.float32(0.02), bc_type=f.bc_type, bc_value=f.bc_value,
+                               flag=flag, solids=solids.cast(np.float32), nthreads=0)
+        m32, p32 = new, m32
+        new, l64 = orc.step_3d(m64, p64, vis_shear=float(np.float32(0.02)), bc_type=f.bc_type, bc_value=f.bc_value,
+                               flag=flag, solids=_solids_from(s).cast(np.float64), dtype=np.float64, nthreads=0)
+        m64, p64 = new, m64
+        got = np.concatenate([f.solid_force.cpu().numpy(), f.solid_torque.cpu().numpy()], axis=1)
+        assert np.abs(got).max() > 0
+        assert _loads_ok(got, l32, l64), (step, got, l32, l64)
+    msgs = orc.check_parity(f.decoded().double().cpu().numpy(), m32, m64)
+    assert not msgs, msgs
