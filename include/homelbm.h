@@ -60,6 +60,8 @@ HL_API const char* hl_version(void);
  *   "d3q27_kernel": 0 automatic, 1 the asynchronous-copy kernel, 2 the TMA-staged kernel
  *   "d3q27_chunks": 0 automatic, k > 0 splits x into k chunks per tile column
  *   "d3q27_stages": 0 automatic (4), 3..5 planes staged by the TMA kernel
+ *   "d3q27_link_blocks": 0 automatic (4 per SM), k > 0 blocks of the cut-link kernel over the
+ *     listed cells (fewer leave SMs free for other domains' kernels on other streams)
  * Returns HL_ERR_ARG for an unknown key. A CUDA graph keeps the choice it was captured with. */
 HL_API int hl_set_tuning(const char* key, int value);
 

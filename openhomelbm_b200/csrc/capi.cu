@@ -12,6 +12,7 @@ static thread_local char g_err[512] = "";
 int g_tune_d3_kernel = 0;
 int g_tune_d3_chunks = 0;
 int g_tune_d3_stages = 0;
+int g_tune_d3_link_blocks = 0;
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -41,6 +42,10 @@ extern "C" int hl_set_tuning(const char* key, int value) {
   }
   if (!strcmp(key, "d3q27_chunks") && value >= 0 && value <= 64) {
     hl::g_tune_d3_chunks = value;
+    return HL_OK;
+  }
+  if (!strcmp(key, "d3q27_link_blocks") && value >= 0 && value <= 4096) {
+    hl::g_tune_d3_link_blocks = value;
     return HL_OK;
   }
   if (!strcmp(key, "d3q27_stages") && (value == 0 || (value >= 3 && value <= 5))) {

@@ -32,12 +32,13 @@
 // binary64 geometry a different boundary, not a more accurate one.)
 //
 // Ray-triangle test: Moller & Trumbore, "Fast, minimum storage ray-triangle intersection"
-// (1997), double-sided, closest hit with 0 <= t <= max_t = 2 (the reference's mesh query
-// bound, lbm_func_3d.py:308), over the triangles that the solid's bin lists for the cell (all
-// of them without bins), screened by the warp against the box the cell's links reach; every
-// lane (direction) then tests the survivors from shared memory. The screen only drops
-// triangles that no lane's exact test could report, so the hits are those of a test against
-// every triangle.
+// (1997), double-sided; a link is cut at the closest hit with 0 <= t <= 1 (the reference's
+// mesh query returns the closest hit up to max_t = 2, lbm_func_3d.py:308, and keeps it when
+// t <= 1). The triangles tested are those the solid's bin lists for the cell (all of them
+// without bins), screened by the warp against the box the cell's links reach, then paired
+// with the directions whose link segment box they meet; each pair is tested by one lane.
+// The screens only drop triangles that cannot be hit with 0 <= t <= 1, so the hits are those
+// of a test against every triangle.
 
 #include <algorithm>
 #include <cmath>
@@ -64,49 +65,32 @@ __device__ __forceinline__ int inverse(int i) { return i == 0 ? 0 : (i & 1) ? i 
 
 using namespace geo;
 
-// Closest double-sided hit 0 <= t <= max_t of the ray o + t d with the triangles tri[list[k]]
-// (k < ntri; list NULL: tri[k]). The caller keeps a hit only when t <= 1, so a triangle whose
-// bounding box misses the box of the segment t in [0, 1] (widened by 1e-3 against rounding)
-// cannot change the outcome and is skipped before the exact test.
-template <class R>
-__device__ bool ray_mesh(const float* tri, const int32_t* list, int ntri, V3<R> o, V3<R> d, R max_t, R* t_out) {
-  bool hit = false;
-  R best = R(0);
-  const float eps = 1e-3f;
-  const float sx0 = float(fmin(o.x, o.x + d.x)) - eps, sx1 = float(fmax(o.x, o.x + d.x)) + eps;
-  const float sy0 = float(fmin(o.y, o.y + d.y)) - eps, sy1 = float(fmax(o.y, o.y + d.y)) + eps;
-  const float sz0 = float(fmin(o.z, o.z + d.z)) - eps, sz1 = float(fmax(o.z, o.z + d.z)) + eps;
-  for (int k = 0; k < ntri; ++k) {
-    const float* v = tri + 9 * (list ? list[k] : k);
-    if (fmaxf(fmaxf(v[0], v[3]), v[6]) < sx0 || fminf(fminf(v[0], v[3]), v[6]) > sx1 ||
-        fmaxf(fmaxf(v[1], v[4]), v[7]) < sy0 || fminf(fminf(v[1], v[4]), v[7]) > sy1 ||
-        fmaxf(fmaxf(v[2], v[5]), v[8]) < sz0 || fminf(fminf(v[2], v[5]), v[8]) > sz1)
-      continue;
-    const R v0x = R(v[0]), v0y = R(v[1]), v0z = R(v[2]);
-    const R e1x = R(v[3]) - v0x, e1y = R(v[4]) - v0y, e1z = R(v[5]) - v0z;
-    const R e2x = R(v[6]) - v0x, e2y = R(v[7]) - v0y, e2z = R(v[8]) - v0z;
-    const R px = d.y * e2z - d.z * e2y, py = d.z * e2x - d.x * e2z, pz = d.x * e2y - d.y * e2x;
-    const R det = e1x * px + e1y * py + e1z * pz;
-    if (det == R(0)) continue;
-    const R inv = R(1) / det;
-    const R sx = o.x - v0x, sy = o.y - v0y, sz = o.z - v0z;
-    const R u = (sx * px + sy * py + sz * pz) * inv;
-    if (u < R(0) || u > R(1)) continue;
-    const R qx = sy * e1z - sz * e1y, qy = sz * e1x - sx * e1z, qz = sx * e1y - sy * e1x;
-    const R w = (d.x * qx + d.y * qy + d.z * qz) * inv;
-    if (w < R(0) || u + w > R(1)) continue;
-    const R t = (e2x * qx + e2y * qy + e2z * qz) * inv;
-    if (t < R(0) || t > max_t) continue;
-    if (!hit || t < best) {
-      best = t;
-      hit = true;
-    }
-  }
-  *t_out = best;
-  return hit;
+// Moller-Trumbore, double-sided: the ray o + t d meets the triangle v[0..8] at t with
+// 0 <= t <= max_t. Binary32, every product and sum rounded on its own (the file is compiled
+// without contraction), as the reference's mesh query computes it.
+__device__ __forceinline__ bool mt_hit(const float* v, V3<float> o, V3<float> d, float max_t, float* t_out) {
+  const float v0x = v[0], v0y = v[1], v0z = v[2];
+  const float e1x = v[3] - v0x, e1y = v[4] - v0y, e1z = v[5] - v0z;
+  const float e2x = v[6] - v0x, e2y = v[7] - v0y, e2z = v[8] - v0z;
+  const float px = d.y * e2z - d.z * e2y, py = d.z * e2x - d.x * e2z, pz = d.x * e2y - d.y * e2x;
+  const float det = e1x * px + e1y * py + e1z * pz;
+  if (det == 0.f) return false;
+  const float inv = 1.f / det;
+  const float sx = o.x - v0x, sy = o.y - v0y, sz = o.z - v0z;
+  const float u = (sx * px + sy * py + sz * pz) * inv;
+  if (u < 0.f || u > 1.f) return false;
+  const float qx = sy * e1z - sz * e1y, qy = sz * e1x - sx * e1z, qz = sx * e1y - sy * e1x;
+  const float w = (d.x * qx + d.y * qy + d.z * qz) * inv;
+  if (w < 0.f || u + w > 1.f) return false;
+  const float t = (e2x * qx + e2y * qy + e2z * qz) * inv;
+  if (t < 0.f || t > max_t) return false;
+  *t_out = t;
+  return true;
 }
 
 template <class R> __device__ __forceinline__ R vlen(R x, R y, R z) { return sqrt(x * x + y * y + z * z); }
+// v / scale, skipping the division for the usual unit scale (where it is exact anyway).
+template <class R> __device__ __forceinline__ R unscale(R v, R scale) { return scale == R(1) ? v : v / scale; }
 
 // mlCalEquilibrium3D_s (lbm_func_3d.py:224-251) for direction (dx, dy, dz) with weight wi.
 template <class R>
@@ -184,7 +168,8 @@ template <class R> __device__ unsigned cut_mask(const hl_solids3d& s, V3<R> cell
     const R sx = R(s.scale_sizes[3 * k]), sy = R(s.scale_sizes[3 * k + 1]), sz = R(s.scale_sizes[3 * k + 2]);
     const int32_t* list;
     int ncand;
-    if (candidates(s, k, ntri, V3<R>{lo.x / sx, lo.y / sy, lo.z / sz}, sx, sy, sz, &list, &ncand))
+    if (candidates(s, k, ntri, V3<R>{unscale(lo.x, sx), unscale(lo.y, sy), unscale(lo.z, sz)}, sx, sy, sz, &list,
+                   &ncand))
       mask |= k < 31 ? (1u << k) : (1u << 31);
   }
   return mask;
@@ -196,6 +181,7 @@ template <class R> __device__ __forceinline__ R warp_sum(R v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+template <class R> __device__ __forceinline__ R lane0(R v) { return __shfl_sync(0xffffffffu, v, 0); }
 __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -204,26 +190,26 @@ __device__ __forceinline__ float warp_max(float v) {
 
 // One near cell with a possible cut link, computed by a whole warp: lane i < 27 rebuilds the
 // population of direction i (a wall population with its momentum exchange if the link is
-// cut, the clamped neighbour population otherwise), the moments are warp sums, and lane 0
-// collides and stores the cell.
-constexpr int MAXC = 64;  // surviving candidate triangles staged per batch, per warp
+// cut, the clamped neighbour population otherwise), the moments are warp sums, and the
+// lanes collide and store the cell (lane k < 10 moment k).
+constexpr unsigned FULL = 0xffffffffu;
+constexpr unsigned NO_HIT = 0xffffffffu;
 
-// Closest hit in [0, 1] over the staged triangles buf[0 .. m) for this lane's ray; updates
-// (cut, sid) when it is nearer than the current one (ties keep the lower solid).
-template <class R>
-__device__ __forceinline__ void test_staged(const float* buf, int m, bool active, V3<R> o, V3<R> d, int k, R& cut,
-                                            int& sid) {
-  R t;
-  if (active && m > 0 && ray_mesh<R>(buf, nullptr, m, o, d, R(2), &t)) {
-    if ((cut < R(0) || t < cut) && t >= R(0) && t <= R(1)) {
-      cut = t;
-      sid = k;
-    }
-  }
-}
+// Per-warp shared scratch of cut_cell, for the solid being tested: per direction its link's
+// segment box in the body frame (min xyz, pad, max xyz, pad; empty for an inactive
+// direction) and ray direction, the current chunk's triangles (slot = lane), the queue of
+// (direction, slot) pairs to test exactly, and per direction the bits of its closest hit.
+struct __align__(16) WarpScratch {
+  float seg[27 * 8];  // read as float4: 16-byte aligned at offset 0 of a 16-byte aligned struct
+  float dir[27 * 3];
+  float tri[32 * 9];
+  unsigned q[32 * 27];
+  unsigned best[32];
+};
+static_assert(sizeof(WarpScratch) % 16 == 0 && alignof(WarpScratch) == 16, "float4 reads of WarpScratch::seg");
 
 template <class S>
-__device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, int z, unsigned mask) {
+__device__ void cut_cell(const Args& a, double* acc, WarpScratch& ws, int x, int y, int z, unsigned mask) {
   using R = typename S::R;
   using T = typename S::T;
   const hl_solids3d& s = a.s;
@@ -231,7 +217,6 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
   const long long N = (long long)nx * ny * nz;
   const long long c = ((long long)x * ny + y) * nz + z;
   const int i = threadIdx.x & 31;
-  const Mom3<R> mc = load_cell<S>(a, N, c);
   R pop = R(0);
   const int ix = i < 27 ? c_cx[i] : 0, iy = i < 27 ? c_cy[i] : 0, iz = i < 27 ? c_cz[i] : 0;
   const R dx = R(ix), dy = R(iy), dz = R(iz);
@@ -247,16 +232,16 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
   // across the warp. The warp screens the candidates 32 at a time (a lane per triangle)
   // against the box that every link of the cell stays in, the cell's body-frame point
   // +- the largest |component| of the lanes' ray directions, widened by 2e-3. That box holds
-  // each lane's segment box of ray_mesh's pre-test (widened by 1e-3), so a triangle outside
-  // it fails every lane's pre-test: dropping it changes no hit. The survivors are staged in
-  // shared memory and every lane tests its own direction against them.
+  // each lane's segment box (widened by 1e-3), so a triangle outside it fails every lane's
+  // segment test: dropping it changes no hit. A survivor is tested exactly only for the
+  // directions whose segment box its bounding box meets (about a tenth of them): those
+  // (direction, triangle) pairs are queued and tested a pair per lane.
   float cut = -1.f;  // geometry in binary32 (see the file comment)
   int sid = -1;
   const V3<R> cell{R(x), R(y), R(z)};
   const V3<R> dir{-dx, -dy, -dz};
   const V3<float> gcell{float(x), float(y), float(z)};
   const V3<float> gdir{-float(ix), -float(iy), -float(iz)};
-  const unsigned lt_mask = (1u << i) - 1u;
   for (int k = 0; k < s.n_objects; ++k) {
     if (!in_mask(mask, k)) continue;  // no candidate triangles for this cell's rays
     const int t0 = s.tri_offset[k], ntri = s.tri_offset[k + 1] - t0;
@@ -268,8 +253,8 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
     const V3<float> lo = xpoint(inv, gcell);
     const V3<float> ld = qrot(inv.qx, inv.qy, inv.qz, inv.qw, gdir);
     const float sx = s.scale_sizes[3 * k], sy = s.scale_sizes[3 * k + 1], sz = s.scale_sizes[3 * k + 2];
-    const V3<float> los{lo.x / sx, lo.y / sy, lo.z / sz};
-    const V3<float> lds{ld.x / sx, ld.y / sy, ld.z / sz};
+    const V3<float> los{unscale(lo.x, sx), unscale(lo.y, sy), unscale(lo.z, sz)};
+    const V3<float> lds{unscale(ld.x, sx), unscale(ld.y, sy), unscale(ld.z, sz)};
     const int32_t* list;
     int ncand;
     if (!candidates(s, k, ntri, los, sx, sy, sz, &list, &ncand)) continue;
@@ -280,7 +265,20 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
     const float by0 = float(los.y) - ry, by1 = float(los.y) + ry;
     const float bz0 = float(los.z) - rz, bz1 = float(los.z) + rz;
     const float* tk = s.tris + 9ll * t0;
-    int nbuf = 0;
+    // this solid's segment boxes and ray directions, one direction per lane
+    const float eps = 1e-3f, inf = __int_as_float(0x7f800000);
+    if (i < 27) {
+      float* sb = ws.seg + 8 * i;
+      sb[0] = active ? fminf(los.x, los.x + lds.x) - eps : inf;
+      sb[1] = active ? fminf(los.y, los.y + lds.y) - eps : inf;
+      sb[2] = active ? fminf(los.z, los.z + lds.z) - eps : inf;
+      sb[4] = active ? fmaxf(los.x, los.x + lds.x) + eps : -inf;
+      sb[5] = active ? fmaxf(los.y, los.y + lds.y) + eps : -inf;
+      sb[6] = active ? fmaxf(los.z, los.z + lds.z) + eps : -inf;
+      ws.dir[3 * i] = lds.x, ws.dir[3 * i + 1] = lds.y, ws.dir[3 * i + 2] = lds.z;
+    }
+    ws.best[i] = NO_HIT;
+    __syncwarp();
     // software pipeline over the chunks: the vertices of chunk q + 1 and the list entries of
     // chunk q + 2 are loaded while chunk q is screened
     auto tri_of = [&](int q) { return list ? __ldg(list + q) : q; };
@@ -301,28 +299,66 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
         for (int j = 0; j < 9; ++j) vn[j] = __ldg(tk + 9 * tri_n + j);
       }
       if (q0 + 64 + i < ncand) tri_n = tri_of(q0 + 64 + i);
-      const bool keep = live && !(fmaxf(fmaxf(v[0], v[3]), v[6]) < bx0 || fminf(fminf(v[0], v[3]), v[6]) > bx1 ||
-                                  fmaxf(fmaxf(v[1], v[4]), v[7]) < by0 || fminf(fminf(v[1], v[4]), v[7]) > by1 ||
-                                  fmaxf(fmaxf(v[2], v[5]), v[8]) < bz0 || fminf(fminf(v[2], v[5]), v[8]) > bz1);
-      const unsigned bal = __ballot_sync(0xffffffffu, keep);
-      const int n = __popc(bal);
-      if (nbuf + n > MAXC) {  // uniform: flush the staged survivors first
-        __syncwarp();
-        test_staged<float>(buf, nbuf, active, los, lds, k, cut, sid);
-        nbuf = 0;
-        __syncwarp();
-      }
+      const float mnx = fminf(fminf(v[0], v[3]), v[6]), mxx = fmaxf(fmaxf(v[0], v[3]), v[6]);
+      const float mny = fminf(fminf(v[1], v[4]), v[7]), mxy = fmaxf(fmaxf(v[1], v[4]), v[7]);
+      const float mnz = fminf(fminf(v[2], v[5]), v[8]), mxz = fmaxf(fmaxf(v[2], v[5]), v[8]);
+      const bool keep = live && !(mxx < bx0 || mnx > bx1 || mxy < by0 || mny > by1 || mxz < bz0 || mnz > bz1);
+      if (__ballot_sync(FULL, keep) == 0u) continue;  // uniform
+      // the directions whose segment box this lane's triangle meets (27 independent tests)
+      unsigned dm = 0u;
       if (keep) {
-        float* dst = buf + 9 * (nbuf + __popc(bal & lt_mask));
+#pragma unroll 9
+        for (int d = 0; d < 27; ++d) {
+          const float4 l4 = *reinterpret_cast<const float4*>(ws.seg + 8 * d);
+          const float4 h4 = *reinterpret_cast<const float4*>(ws.seg + 8 * d + 4);
+          if (!(mxx < l4.x || mnx > h4.x || mxy < l4.y || mny > h4.y || mxz < l4.z || mnz > h4.z)) dm |= 1u << d;
+        }
+        if (dm) {
 #pragma unroll
-        for (int j = 0; j < 9; ++j) dst[j] = v[j];
+          for (int j = 0; j < 9; ++j) ws.tri[9 * i + j] = v[j];
+        }
       }
-      nbuf += n;
+      // queue the (direction, slot) pairs: exclusive scan of the lanes' counts
+      const int cnt = __popc(dm);
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, incl, o);
+        if (i >= o) incl += t;
+      }
+      const int total = __shfl_sync(FULL, incl, 31);
+      int off = incl - cnt;
+      for (unsigned b = dm; b; b &= b - 1u) ws.q[off++] = (unsigned(__ffs(b) - 1) << 5) | unsigned(i);
+      __syncwarp();
+      // the exact tests, a pair per lane; a hit with 0 <= t <= 1 lowers best[direction]
+      for (int p0 = 0; p0 < total; p0 += 32) {
+        if (p0 + i < total) {
+          const unsigned e = ws.q[p0 + i];
+          const int d = int(e >> 5);
+          const V3<float> dd{ws.dir[3 * d], ws.dir[3 * d + 1], ws.dir[3 * d + 2]};
+          float t;
+          if (mt_hit(ws.tri + 9 * (e & 31u), los, dd, 1.f, &t))
+            atomicMin(&ws.best[d], t == 0.f ? 0u : __float_as_uint(t));
+        }
+      }
+      __syncwarp();
     }
     __syncwarp();
-    test_staged<float>(buf, nbuf, active, los, lds, k, cut, sid);
-    __syncwarp();
+    // this solid's closest hit per direction; ties keep the lower solid
+    const unsigned bt = ws.best[i];
+    if (bt != NO_HIT) {
+      const float t = __uint_as_float(bt);
+      if (cut < 0.f || t < cut) {
+        cut = t;
+        sid = k;
+      }
+    }
   }
+  // no cut link: the cell keeps the plain kernel's result (the same arithmetic on plain links)
+  if (__ballot_sync(FULL, sid >= 0) == 0u) return;
+  // the cell's own moments, loaded after the ray tests (they are not needed there and would
+  // hold registers through them); an uncut lane's neighbour load below overlaps this one
+  const Mom3<R> mc = load_cell<S>(a, N, c);
   double lf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // this link's momentum exchange and torque
   if (active) {
     const R wi = weight<R>(i);
@@ -387,12 +423,15 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
   }
   // moments (lbm_func_3d.py:528-562) as warp sums: rho, the signed first moments and the
   // second moments (c_a^2 = |c_a|)
-  const R rho = warp_sum(pop);
-  const R jx = warp_sum(R(ix) * pop), jy = warp_sum(R(iy) * pop), jz = warp_sum(R(iz) * pop);
-  const R pxx = warp_sum(R(ix * ix) * pop), pyy = warp_sum(R(iy * iy) * pop), pzz = warp_sum(R(iz * iz) * pop);
-  R pixy = warp_sum(R(ix * iy) * pop), pixz = warp_sum(R(ix * iz) * pop), piyz = warp_sum(R(iy * iz) * pop);
-  if (i != 0) return;
-  // regularised collision (564-604)
+  // (the butterfly sums can differ between lanes in the last bit; every lane takes lane 0's)
+  const R rho = lane0(warp_sum(pop));
+  const R jx = lane0(warp_sum(R(ix) * pop)), jy = lane0(warp_sum(R(iy) * pop)), jz = lane0(warp_sum(R(iz) * pop));
+  const R pxx = lane0(warp_sum(R(ix * ix) * pop)), pyy = lane0(warp_sum(R(iy * iy) * pop));
+  const R pzz = lane0(warp_sum(R(iz * iz) * pop));
+  R pixy = lane0(warp_sum(R(ix * iy) * pop)), pixz = lane0(warp_sum(R(ix * iz) * pop));
+  R piyz = lane0(warp_sum(R(iy * iz) * pop));
+  // regularised collision (564-604), the same in every lane; lane k < 10 encodes and stores
+  // moment k
   const R Fx = a.w.force ? R(a.w.force[c]) : R(0);
   const R Fy = a.w.force ? R(a.w.force[N + c]) : R(0);
   const R Fz = a.w.force ? R(a.w.force[2 * N + c]) : R(0);
@@ -431,9 +470,11 @@ __device__ void cut_cell(const Args& a, double* acc, float* buf, int x, int y, i
   m.syz = piyz * invRho;
   R raw[10];
   encode3<S>(m, a.sc, raw);
-  T* post = static_cast<T*>(a.w.post);
+  R mine = raw[0];
 #pragma unroll
-  for (int k = 0; k < 10; ++k) post[k * N + c] = S::from_r(raw[k], unsigned(k * N + c));
+  for (int k = 1; k < 10; ++k)
+    if (i == k) mine = raw[k];
+  if (i < 10) static_cast<T*>(a.w.post)[i * N + c] = S::from_r(mine, unsigned(i * N + c));
 }
 
 template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __grid_constant__ Args a) {
@@ -470,7 +511,7 @@ template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __
     flagged = solids != 0u;
   }
   // 2. the warp computes its flagged cells one after another, a lane per direction
-  __shared__ float tri_buf[BLOCK / 32][MAXC * 9];
+  __shared__ WarpScratch scratch[BLOCK / 32];
   unsigned mask = __ballot_sync(0xffffffffu, flagged);
   const bool any = mask != 0;
   while (mask) {
@@ -479,7 +520,7 @@ template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __
     const int cx = __shfl_sync(0xffffffffu, x, src), cy = __shfl_sync(0xffffffffu, y, src),
               cz = __shfl_sync(0xffffffffu, z, src);
     const unsigned cm = __shfl_sync(0xffffffffu, solids, src);
-    cut_cell<S>(a, acc, tri_buf[threadIdx.x >> 5], cx, cy, cz, cm);
+    cut_cell<S>(a, acc, scratch[threadIdx.x >> 5], cx, cy, cz, cm);
     __syncwarp();
   }
   if (!__syncthreads_or(any)) return;
@@ -487,9 +528,13 @@ template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __
     if (acc[k] != 0.0) atomicAdd(&s.loads64[k], acc[k]);
 }
 
-// Work-list form. classify_kernel: one thread per box cell appends the cells that can have a
-// cut link to work[1..] (count in work[0], one atomic per warp); process_kernel: a fixed grid
-// of warps takes the listed cells in turn, a cell per warp as in band_kernel.
+// Work-list form. The int32 scratch holds a header of WORK_HEAD ints (listed cells, finished
+// process blocks, next cell to take, unused), zeroed before each call, then (cell, solid
+// mask) pairs. classify_kernel: one thread per box cell appends the cells that can have a cut
+// link (one atomic per warp); process_kernel: a fixed grid of warps takes the listed cells
+// one at a time from a shared counter, a cell per warp as in band_kernel, so that a warp held
+// by an expensive cell (near a joint, hundreds of candidate triangles) takes no others.
+constexpr int WORK_HEAD = 4;
 template <class S> __global__ void __launch_bounds__(BLOCK) classify_kernel(const __grid_constant__ Args a) {
   using R = typename S::R;
   const hl_solids3d& s = a.s;
@@ -523,8 +568,8 @@ template <class S> __global__ void __launch_bounds__(BLOCK) classify_kernel(cons
   base = __shfl_sync(0xffffffffu, base, leader);
   if (flagged) {
     const int slot = base + __popc(mask & ((1u << lane) - 1));
-    s.work[2 + 2 * slot] = c;
-    s.work[3 + 2 * slot] = int(solids);
+    s.work[WORK_HEAD + 2 * slot] = c;
+    s.work[WORK_HEAD + 1 + 2 * slot] = int(solids);
   }
 }
 
@@ -537,8 +582,7 @@ __device__ __forceinline__ void loads_out(const hl_solids3d& s, int k) {
   }
 }
 
-// The block that finishes last (work[1] counts finished blocks; zeroed before the launch)
-// writes the binary32 loads.
+// The block that finishes last (work[1] counts finished blocks) writes the binary32 loads.
 template <class S> __global__ void __launch_bounds__(BLOCK) process_kernel(const __grid_constant__ Args a) {
   __shared__ double acc[MAX_SOLIDS * 6];
   __shared__ bool last;
@@ -546,16 +590,19 @@ template <class S> __global__ void __launch_bounds__(BLOCK) process_kernel(const
   const int n = s.n_objects;
   for (int k = threadIdx.x; k < 6 * n; k += blockDim.x) acc[k] = 0.0;
   __syncthreads();
-  __shared__ float tri_buf[BLOCK / 32][MAXC * 9];
+  __shared__ WarpScratch scratch[BLOCK / 32];
   const int count = s.work[0];
-  const int warps = gridDim.x * (BLOCK / 32);
   const int ny = a.w.ny, nz = a.w.nz;
   bool any = false;
-  for (int j = blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5); j < count; j += warps) {
-    const int c = s.work[2 + 2 * j];
-    const unsigned cm = unsigned(s.work[3 + 2 * j]);
+  for (;;) {
+    int j = 0;
+    if ((threadIdx.x & 31) == 0) j = atomicAdd(s.work + 2, 1);
+    j = __shfl_sync(FULL, j, 0);
+    if (j >= count) break;
+    const int c = s.work[WORK_HEAD + 2 * j];
+    const unsigned cm = unsigned(s.work[WORK_HEAD + 1 + 2 * j]);
     any = true;
-    cut_cell<S>(a, acc, tri_buf[threadIdx.x >> 5], c / (ny * nz), (c / nz) % ny, c % nz, cm);
+    cut_cell<S>(a, acc, scratch[threadIdx.x >> 5], c / (ny * nz), (c / nz) % ny, c % nz, cm);
     __syncwarp();
   }
   if (__syncthreads_or(any)) {
@@ -600,15 +647,14 @@ template <class S> int launch(const hl_world3d* w, double vis, const hl_solids3d
   const long long cells = (long long)a.box_side * a.box_side * a.box_side;
   const dim3 grid(unsigned((cells + BLOCK - 1) / BLOCK), unsigned(s->n_objects));
   if (s->work != nullptr) {
-    // work[0]: listed cells, work[1]: finished process blocks
-    cudaError_t e = cudaMemsetAsync(s->work, 0, 2 * sizeof(int32_t), st);
+    cudaError_t e = cudaMemsetAsync(s->work, 0, WORK_HEAD * sizeof(int32_t), st);
     if (e != cudaSuccess) return cuda_status(e, "d3q27 solid links: zero work count");
     classify_kernel<S><<<grid, BLOCK, 0, st>>>(a);
     HL_LAUNCH_CHECK("d3q27 solid links (classify)");
-    // four blocks per SM take the listed cells in turn (measured: smaller grids leave the
-    // densely listed bands of small domains to too few warps); the last block to finish
-    // writes the binary32 loads
-    process_kernel<S><<<unsigned(4 * num_sms_local()), BLOCK, 0, st>>>(a);
+    // four blocks per SM, as many as the registers allow (measured: 6 or 8 with fewer
+    // registers spill and run no faster); the last block to finish writes the binary32 loads
+    const int blocks = g_tune_d3_link_blocks > 0 ? g_tune_d3_link_blocks : 4 * num_sms_local();
+    process_kernel<S><<<unsigned(blocks), BLOCK, 0, st>>>(a);
     HL_LAUNCH_CHECK("d3q27 solid links (cut cells)");
   } else {
     band_kernel<S><<<grid, BLOCK, 0, st>>>(a);
@@ -653,6 +699,6 @@ extern "C" int hl_d3q27_solid_links(const hl_world3d* w, double vis_shear, const
 extern "C" size_t hl_d3q27_solid_links_work_ints(int n_objects, float max_bound_radius) {
   if (n_objects <= 0 || !(max_bound_radius >= 0.f) || max_bound_radius >= 512.f) return 0;
   const size_t side = size_t(d3s::box_side_of(max_bound_radius));
-  // count, finished-block counter, then (cell, solid mask) pairs
-  return 2 + 2 * size_t(n_objects) * side * side * side;
+  // header (listed cells, finished blocks, next cell, unused), then (cell, solid mask) pairs
+  return d3s::WORK_HEAD + 2 * size_t(n_objects) * side * side * side;
 }

@@ -16,6 +16,7 @@ int cuda_status(cudaError_t e, const char* what);
 extern int g_tune_d3_kernel;  // hl_set_tuning("d3q27_kernel")
 extern int g_tune_d3_chunks;  // hl_set_tuning("d3q27_chunks")
 extern int g_tune_d3_stages;  // hl_set_tuning("d3q27_stages")
+extern int g_tune_d3_link_blocks;  // hl_set_tuning("d3q27_link_blocks")
 
 #define HL_CHECK_ARG(cond, ...)       \
   do {                                \
