@@ -503,6 +503,9 @@ def run_serve(args):
     torch.cuda.synchronize()
     plain = serving.run_plain(reqs, storage="float32")
     served = serving.ServeEngine(storage="float16", max_active=args.slots, budget_bytes=150e9).run(reqs)
+    # the same requests with one stream-collide launch per substep over all active domains
+    batched = serving.ServeEngine(storage="float16", max_active=args.slots, budget_bytes=150e9,
+                                  batched=True).run(reqs)
     # agreement of the served float16 loads with the plain float32 loads, request by request
     errs = []
     for r in reqs:
@@ -529,6 +532,8 @@ def run_serve(args):
                        "p99_ms": served.pct(99) * 1e3, "p99_over_p50": served.pct(99) / served.pct(50),
                        "wall_s": served.wall_s, "max_active": served.max_active,
                        "mlups": cells / served.wall_s / 1e6},
+            "served_batched_stream_collide": {"env_steps_per_s": batched.env_steps_per_s,
+                                              "p50_ms": batched.pct(50) * 1e3, "p99_ms": batched.pct(99) * 1e3},
             "plain": {"env_steps_per_s": plain.env_steps_per_s, "p50_ms": plain.pct(50) * 1e3,
                       "p99_ms": plain.pct(99) * 1e3, "wall_s": plain.wall_s, "mlups": cells / plain.wall_s / 1e6},
             "loads_rel_l2_f16_vs_plain_f32": {"median": float(np.median(errs)), "max": float(np.max(errs))},

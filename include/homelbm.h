@@ -145,6 +145,27 @@ HL_API size_t hl_d3q27_scratch_bytes(const hl_world3d* w);
  *    other host threads) race on the array: serialise them. */
 HL_API int hl_d3q27_stream_collide_noalloc(const hl_world3d* w, double vis_shear, double* mass, int32_t* health,
                                            hl_stream stream);
+
+/* Batched domains (the serving form; no reference counterpart: the reference launches each
+ * LBM_Solver3D's step on its own, envs/lbm3d/lbm_solver_3d.py:88-127). One stream-collide
+ * launch steps many walled domains of different sizes: the tiles of all of them form one item
+ * sequence that the CTAs share, so small domains do not leave SMs idle.
+ *  - hl_d3q27_batch_bytes: device bytes of the descriptors of n domains.
+ *  - hl_d3q27_batch_prepare: writes the descriptors of worlds[0 .. n) into desc (device
+ *    memory, 64-byte aligned): buffers (parity 0 reads cur, parity 1 reads post), sizes, x
+ *    split and tensor maps. Every world walled, without force or flag fields, TMA-eligible
+ *    (ny % 16 == 0, nz % 32 == 0, 16-byte aligned buffers), float32/float16/bfloat16, one
+ *    storage type and scale for all. Sets *n_items. Synchronises the stream (not for stream
+ *    capture); prepare again after any domain's buffers change.
+ *  - hl_d3q27_stream_collide_batch: one stream-collide of every domain of desc at parity p
+ *    (reads buffer p, writes buffer p ^ 1); per cell the same result as
+ *    hl_d3q27_stream_collide. n_domains and n_items must be those of the prepare call.
+ *    Capturable. status (or NULL) is set to HL_ERR_TIMEOUT if a bounded wait gave up. */
+HL_API size_t hl_d3q27_batch_bytes(int n_domains);
+HL_API int hl_d3q27_batch_prepare(const hl_world3d* worlds, int n_domains, void* desc, size_t desc_bytes,
+                                  int* n_items, hl_stream stream);
+HL_API int hl_d3q27_stream_collide_batch(const void* desc, int n_domains, int n_items, double vis_shear,
+                                         const hl_storage* storage, int parity, int* status, hl_stream stream);
 HL_API size_t hl_d3q27_bc_scratch_bytes(const hl_world3d* w);
 
 /* Replaces InitFlow3D (envs/lbm3d/lbm_func_3d.py:22-83) and set_uniform_flow_3d_kernel

@@ -36,6 +36,8 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <algorithm>
+#include <vector>
 
 #include "d3q27_core.cuh"
 #include "d3q27_pair.cuh"
@@ -80,6 +82,16 @@ struct Maps {
   CUtensorMap mid, yedge, zedge, corner;  // over the current buffer
 };
 
+// One domain of a batched launch (device memory, 64-byte aligned like the maps in it): the
+// tensor maps over each of its two buffers (parity p reads buf[p] and writes buf[p ^ 1]), its
+// sizes and x split, and the first of its items in the batch's item sequence.
+struct BatchDomain {
+  Maps maps[2];
+  void* buf[2];
+  long long N;
+  int nx, ny, nz, tiles_z, n_tiles, chunk_len, n_items, item_base;
+};
+
 
 
 // ---------------------------------------------------------------- PTX helpers
@@ -110,6 +122,12 @@ __device__ __forceinline__ void tma_load4(unsigned dst, const CUtensorMap* map, 
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+// Tensor maps read from global memory: make the copy written before the launch visible to the
+// tensor-map proxy before the first copy through it.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* m) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(reinterpret_cast<unsigned long long>(m))
+               : "memory");
+}
 
 // ---------------------------------------------------------------- kernel
 // Mailbox slot of direction (xi, yi, zi) with (yi, zi) != (1, 1): the populations a
@@ -218,8 +236,14 @@ __device__ __forceinline__ void load_raw(const typename S::T* p0, const typename
   }
 }
 
-template <class S, int NSTAGE, bool PERIODIC, bool FORCE, bool FLAGS, bool DIAG>
-__global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, const __grid_constant__ Maps maps) {
+// BATCH: the items belong to the domains of doms[0 .. n_doms) (their item ranges in order);
+// a's sizes, buffers and item count are unused except n_items (the batch's total), and each
+// item takes its domain's sizes, buffers and maps at parity `parity`. Walled domains only.
+template <class S, int NSTAGE, bool PERIODIC, bool FORCE, bool FLAGS, bool DIAG, bool BATCH>
+__global__ void __launch_bounds__(THREADS, 1)
+    step_kernel_tma(const StepArgs a, const __grid_constant__ Maps maps, const BatchDomain* __restrict__ doms,
+                    int n_doms, int parity) {
+  static_assert(!BATCH || (!PERIODIC && !FORCE && !FLAGS && !DIAG), "batched launches: walled domains, no fields");
   using T = typename S::T;
   static_assert(sizeof(typename S::R) == 4, "the paired kernel computes in binary32");
   using G = Geo<T, NSTAGE>;
@@ -278,8 +302,10 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
     h_ok[i] = has_halo && ddy >= 0 && ddy < TY && ddz >= 0 && ddz < TZ;
     h_dst[i] = ddy * TZ + ddz;
   }
-  const long long N = a.N;
-  const long long plane = (long long)a.ny * a.nz;
+  // the current item's domain (fixed for a single-domain launch)
+  long long N = a.N;
+  long long plane = (long long)a.ny * a.nz;
+  int nx = a.nx, ny = a.ny, nz = a.nz;
   T* post = static_cast<T*>(a.post);
   const PairConst kc = make_pair_const(1.f / (float(a.vis_shear) * 3.f + 0.5f));
 
@@ -298,13 +324,49 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
   // consumers, across item boundaries, so a new item starts with its planes already staged.
   int slot = 0, phase = 0;                                  // consumer position
   int p_item = blockIdx.x, p_x = 0, p_xe = 0, p_slot = 0;  // producer position (thread 0)
-  int p_y0 = 0, p_z0 = 0;
-  auto item_range = [&](int item, int& y0, int& z0, int& xb, int& xe) {
-    const int tile = item % a.n_tiles, chunk = item / a.n_tiles;
-    y0 = (tile / a.tiles_z) * TY;
-    z0 = (tile % a.tiles_z) * TZ;
-    xb = chunk * a.chunk_len;
-    xe = min(xb + a.chunk_len, a.nx);
+  int p_y0 = 0, p_z0 = 0, p_dom = -1;
+  const Maps* p_maps = &maps;
+  // the domain of a batch item: the last one whose item range starts at or before it
+  auto find_dom = [&](int item) {
+    int lo = 0, hi = n_doms - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (doms[mid].item_base <= item) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  };
+  auto item_range = [&](int item, int& y0, int& z0, int& xb, int& xe, int& dom) {
+    if constexpr (BATCH) {
+      dom = find_dom(item);
+      const BatchDomain& D = doms[dom];
+      const int local = item - D.item_base;
+      const int tile = local % D.n_tiles, chunk = local / D.n_tiles;
+      y0 = (tile / D.tiles_z) * TY;
+      z0 = (tile % D.tiles_z) * TZ;
+      xb = chunk * D.chunk_len;
+      xe = min(xb + D.chunk_len, D.nx);
+    } else {
+      dom = 0;
+      const int tile = item % a.n_tiles, chunk = item / a.n_tiles;
+      y0 = (tile / a.tiles_z) * TY;
+      z0 = (tile % a.tiles_z) * TZ;
+      xb = chunk * a.chunk_len;
+      xe = min(xb + a.chunk_len, a.nx);
+    }
+  };
+  // thread 0: the maps of the producer's current item (batch: acquired once per domain change)
+  auto producer_maps = [&](int dom) {
+    if constexpr (BATCH) {
+      if (dom != p_dom) {
+        p_dom = dom;
+        p_maps = &doms[dom].maps[parity];
+        tensormap_acquire(&p_maps->mid);
+        tensormap_acquire(&p_maps->yedge);
+        tensormap_acquire(&p_maps->zedge);
+        tensormap_acquire(&p_maps->corner);
+      }
+    }
   };
   auto issue = [&](int xs, int q_slot, int y0, int z0) {
     // nine boxes of plane xs of the tile at (y0, z0) into stage q_slot
@@ -321,15 +383,16 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
     }
     fence_proxy_async();
     mbar_expect_tx(bar, G::TX_BYTES);
-    tma_load4(saddr(st + G::OFF_MID), &maps.mid, z0, y0, gx, 0, bar);
-    tma_load4(saddr(st + G::OFF_YLO), &maps.yedge, z0, yl, gx, 0, bar);
-    tma_load4(saddr(st + G::OFF_YHI), &maps.yedge, z0, yh, gx, 0, bar);
-    tma_load4(saddr(st + G::OFF_ZLO), &maps.zedge, zl, y0, gx, 0, bar);
-    tma_load4(saddr(st + G::OFF_ZHI), &maps.zedge, zh, y0, gx, 0, bar);
-    tma_load4(saddr(st + G::OFF_C + 0 * G::B_C), &maps.corner, zl, yl, gx, 0, bar);
-    tma_load4(saddr(st + G::OFF_C + 1 * G::B_C), &maps.corner, zh, yl, gx, 0, bar);
-    tma_load4(saddr(st + G::OFF_C + 2 * G::B_C), &maps.corner, zl, yh, gx, 0, bar);
-    tma_load4(saddr(st + G::OFF_C + 3 * G::B_C), &maps.corner, zh, yh, gx, 0, bar);
+    const Maps& m = *p_maps;
+    tma_load4(saddr(st + G::OFF_MID), &m.mid, z0, y0, gx, 0, bar);
+    tma_load4(saddr(st + G::OFF_YLO), &m.yedge, z0, yl, gx, 0, bar);
+    tma_load4(saddr(st + G::OFF_YHI), &m.yedge, z0, yh, gx, 0, bar);
+    tma_load4(saddr(st + G::OFF_ZLO), &m.zedge, zl, y0, gx, 0, bar);
+    tma_load4(saddr(st + G::OFF_ZHI), &m.zedge, zh, y0, gx, 0, bar);
+    tma_load4(saddr(st + G::OFF_C + 0 * G::B_C), &m.corner, zl, yl, gx, 0, bar);
+    tma_load4(saddr(st + G::OFF_C + 1 * G::B_C), &m.corner, zh, yl, gx, 0, bar);
+    tma_load4(saddr(st + G::OFF_C + 2 * G::B_C), &m.corner, zl, yh, gx, 0, bar);
+    tma_load4(saddr(st + G::OFF_C + 3 * G::B_C), &m.corner, zh, yh, gx, 0, bar);
   };
   auto produce = [&](int n) {  // thread 0: the next n planes of the sequence
     for (int k = 0; k < n && p_item < a.n_items; ++k) {
@@ -338,16 +401,18 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
       if (++p_x > p_xe) {
         p_item += gridDim.x;
         if (p_item < a.n_items) {
-          int xb;
-          item_range(p_item, p_y0, p_z0, xb, p_xe);
+          int xb, dom;
+          item_range(p_item, p_y0, p_z0, xb, p_xe, dom);
+          producer_maps(dom);
           p_x = xb - 1;
         }
       }
     }
   };
   if (tid == 0 && p_item < a.n_items) {
-    int xb;
-    item_range(p_item, p_y0, p_z0, xb, p_xe);
+    int xb, dom;
+    item_range(p_item, p_y0, p_z0, xb, p_xe, dom);
+    producer_maps(dom);
     p_x = xb - 1;
     produce(NSTAGE);
   }
@@ -363,10 +428,19 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
   };
 
   for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
-    int y0, z0, xb, xe;
-    item_range(item, y0, z0, xb, xe);
+    int y0, z0, xb, xe, dom;
+    item_range(item, y0, z0, xb, xe, dom);
+    if constexpr (BATCH) {
+      const BatchDomain& D = doms[dom];
+      N = D.N;
+      nx = D.nx;
+      ny = D.ny;
+      nz = D.nz;
+      plane = (long long)D.ny * D.nz;
+      post = static_cast<T*>(D.buf[parity ^ 1]);
+    }
     const int hgy = y0 - 1 + hsy, hgz = z0 - 1 + hsz;
-    const bool h_in = PERIODIC || (hgy >= 0 && hgy < a.ny && hgz >= 0 && hgz < a.nz);
+    const bool h_in = PERIODIC || (hgy >= 0 && hgy < ny && hgz >= 0 && hgz < nz);
     const int dy = y0 + ty, dz = z0 + tz;
     // group sums of the previous pair that the next destinations still need: all of c_x = +1,
     // the second plane's of c_x = 0
@@ -388,8 +462,8 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
       }
       wait_stage(slot0, ph0);
       if (has1) wait_stage(slot1, ph1);
-      const bool in0 = PERIODIC || (s0 >= 0 && s0 < a.nx);
-      const bool in1 = has1 && (PERIODIC || (s1 >= 0 && s1 < a.nx));
+      const bool in0 = PERIODIC || (s0 >= 0 && s0 < nx);
+      const bool in1 = has1 && (PERIODIC || (s1 >= 0 && s1 < nx));
       const unsigned char* st0 = smem + slot0 * G::STAGE_BYTES;
       const unsigned char* st1 = smem + slot1 * G::STAGE_BYTES;
 
@@ -467,15 +541,15 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel_tma(const StepArgs a, 
       const int d0 = s0 - 1;
       const bool v0 = d0 >= xb && d0 < xe, v1 = d0 + 1 >= xb && d0 + 1 < xe;
       if (v0 || v1) {
-        const long long c0 = (long long)d0 * plane + (long long)dy * a.nz + dz, c1 = c0 + plane;
+        const long long c0 = (long long)d0 * plane + (long long)dy * nz + dz, c1 = c0 + plane;
         bool f0 = v0, f1 = v1;
         if (FLAGS) {
           f0 = f0 && a.flag[c0] == ML_FLUID;
           f1 = f1 && a.flag[c1] == ML_FLUID;
         } else if (!PERIODIC) {
-          const bool yz = dy > 0 && dy < a.ny - 1 && dz > 0 && dz < a.nz - 1;
-          f0 = f0 && yz && d0 > 0 && d0 < a.nx - 1;
-          f1 = f1 && yz && d0 + 1 > 0 && d0 + 1 < a.nx - 1;
+          const bool yz = dy > 0 && dy < ny - 1 && dz > 0 && dz < nz - 1;
+          f0 = f0 && yz && d0 > 0 && d0 < nx - 1;
+          f1 = f1 && yz && d0 + 1 > 0 && d0 + 1 < nx - 1;
         }
         if (f0 || f1) {
           P2 Fx(0.f, 0.f), Fy(0.f, 0.f), Fz(0.f, 0.f);
@@ -643,7 +717,7 @@ int launch(const hl_world3d* w, double vis, const hl_diag* diag, cudaStream_t st
   a.flag = w->flag;
   a.sc = make_scale(w->storage);
   if (DIAG) fill_diag(a, diag);
-  auto kern = step_kernel_tma<S, NSTAGE, PERIODIC, FORCE, FLAGS, DIAG>;
+  auto kern = step_kernel_tma<S, NSTAGE, PERIODIC, FORCE, FLAGS, DIAG, false>;
   {
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
@@ -661,7 +735,7 @@ int launch(const hl_world3d* w, double vis, const hl_diag* diag, cudaStream_t st
     attr = true;
   }
   const int grid = a.n_items < sms ? a.n_items : sms;
-  kern<<<grid, THREADS, G::SMEM, st>>>(a, maps);
+  kern<<<grid, THREADS, G::SMEM, st>>>(a, maps, nullptr, 0, 0);
   HL_LAUNCH_CHECK("d3q27 stream_collide (tma) launch");
   return HL_OK;
 }
@@ -686,6 +760,37 @@ template <class S, int NS> int dispatch(const hl_world3d* w, double vis, const h
 #undef HL_T_CASE
   set_error("d3q27 (tma): unsupported option combination");
   return HL_ERR_UNSUPPORTED;
+}
+
+// ---------------------------------------------------------------- batched domains
+// Prepared descriptor arrays (device address -> domains, items), so that a launch can only
+// use counts that match what was written there.
+std::mutex g_batch_mu;
+std::map<const void*, std::pair<int, int>> g_batches;
+
+template <class S, int NSTAGE>
+int launch_batch(const BatchDomain* doms, int n_doms, int n_items, double vis, const hl_storage& storage, int parity,
+                 int* status, cudaStream_t st) {
+  using G = Geo<typename S::T, NSTAGE>;
+  StepArgs a{};
+  a.n_items = n_items;
+  a.vis_shear = vis;
+  a.sc = make_scale(storage);
+  a.status = status;
+  Maps maps;
+  std::memset(&maps, 0, sizeof(maps));
+  auto kern = step_kernel_tma<S, NSTAGE, false, false, false, false, true>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(d3q27 tma batch)");
+    attr = true;
+  }
+  const int sms = num_sms();
+  const int grid = n_items < sms ? n_items : sms;
+  kern<<<grid, THREADS, G::SMEM, st>>>(a, maps, doms, n_doms, parity);
+  HL_LAUNCH_CHECK("d3q27 stream_collide (tma batch) launch");
+  return HL_OK;
 }
 
 }  // namespace tma
@@ -722,3 +827,96 @@ int launch_step_tma(const hl_world3d* w, double vis, const hl_diag* diag, cudaSt
 
 }  // namespace d3
 }  // namespace hl
+
+using namespace hl;
+
+extern "C" size_t hl_d3q27_batch_bytes(int n_domains) {
+  return n_domains > 0 ? size_t(n_domains) * sizeof(d3::tma::BatchDomain) : 0;
+}
+
+extern "C" int hl_d3q27_batch_prepare(const hl_world3d* worlds, int n_domains, void* desc, size_t desc_bytes,
+                                      int* n_items, hl_stream stream) {
+  using d3::tma::BatchDomain;
+  HL_CHECK_ARG(worlds != nullptr && n_items != nullptr, "d3q27 batch: worlds or n_items is NULL");
+  HL_CHECK_ARG(n_domains >= 1 && n_domains <= 4096, "d3q27 batch: %d domains (1 .. 4096)", n_domains);
+  HL_CHECK_ARG(desc != nullptr && (reinterpret_cast<uintptr_t>(desc) & 63) == 0,
+               "d3q27 batch: descriptor buffer NULL or not 64-byte aligned");
+  HL_CHECK_ARG(desc_bytes >= hl_d3q27_batch_bytes(n_domains), "d3q27 batch: descriptor buffer too small (%zu < %zu)",
+               desc_bytes, hl_d3q27_batch_bytes(n_domains));
+  const hl_world3d& w0 = worlds[0];
+  HL_CHECK_ARG(w0.storage.dtype == HL_F32 || w0.storage.dtype == HL_F16 || w0.storage.dtype == HL_BF16,
+               "d3q27 batch: storage dtype %d (float32, float16 or bfloat16)", int(w0.storage.dtype));
+  std::vector<BatchDomain> h;
+  h.resize(size_t(n_domains));
+  long long total = 0;
+  for (int k = 0; k < n_domains; ++k) {
+    const hl_world3d& w = worlds[k];
+    HL_CHECK_ARG(w.nx >= 3 && w.ny >= 3 && w.nz >= 3, "d3q27 batch: domain %d has dims %d x %d x %d", k, w.nx, w.ny,
+                 w.nz);
+    HL_CHECK_ARG(w.cur != nullptr && w.post != nullptr && w.cur != w.post, "d3q27 batch: domain %d buffers", k);
+    HL_CHECK_ARG(d3::tma_eligible(&w), "d3q27 batch: domain %d is not TMA-eligible (ny %% 16, nz %% 32, alignment)",
+                 k);
+    HL_CHECK_ARG(!w.periodic && w.force == nullptr && w.flag == nullptr,
+                 "d3q27 batch: domain %d must be walled, without force or flag fields", k);
+    HL_CHECK_ARG(w.storage.dtype == w0.storage.dtype && w.storage.u_scale == w0.storage.u_scale &&
+                     w.storage.s_scale == w0.storage.s_scale,
+                 "d3q27 batch: domain %d has another storage type or scale than domain 0", k);
+    BatchDomain& d = h[size_t(k)];
+    hl_world3d flip = w;
+    flip.cur = w.post;
+    flip.post = const_cast<void*>(w.cur);
+    int rc = d3::tma::encode_maps(&w, &d.maps[0]);
+    if (rc != HL_OK) return rc;
+    rc = d3::tma::encode_maps(&flip, &d.maps[1]);
+    if (rc != HL_OK) return rc;
+    d.buf[0] = const_cast<void*>(w.cur);
+    d.buf[1] = w.post;
+    d.N = (long long)w.nx * w.ny * w.nz;
+    d.nx = w.nx;
+    d.ny = w.ny;
+    d.nz = w.nz;
+    d.tiles_z = w.nz / d3::tma::TZ;
+    d.n_tiles = (w.ny / d3::tma::TY) * d.tiles_z;
+    // x chunks of about 32 planes: with the items of every domain to spread over the SMs,
+    // the chunks only need to be long against the two halo planes each one reads
+    const int chunks = std::max(1, (w.nx + 16) / 32);
+    d.chunk_len = (w.nx + chunks - 1) / chunks;
+    d.n_items = d.n_tiles * ((w.nx + d.chunk_len - 1) / d.chunk_len);
+    d.item_base = int(total);
+    total += d.n_items;
+    HL_CHECK_ARG(total < (1ll << 30), "d3q27 batch: too many items");
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemcpyAsync(desc, h.data(), h.size() * sizeof(BatchDomain), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(e, "d3q27 batch: descriptor upload");
+  {
+    std::lock_guard<std::mutex> lk(d3::tma::g_batch_mu);
+    d3::tma::g_batches[desc] = {n_domains, int(total)};
+  }
+  *n_items = int(total);
+  return HL_OK;
+}
+
+extern "C" int hl_d3q27_stream_collide_batch(const void* desc, int n_domains, int n_items, double vis_shear,
+                                             const hl_storage* storage, int parity, int* status, hl_stream stream) {
+  HL_CHECK_ARG(desc != nullptr && storage != nullptr, "d3q27 batch: descriptors or storage is NULL");
+  HL_CHECK_ARG(vis_shear > 0.0, "d3q27 batch: viscosity must be positive");
+  HL_CHECK_ARG(parity == 0 || parity == 1, "d3q27 batch: parity %d", parity);
+  {
+    std::lock_guard<std::mutex> lk(d3::tma::g_batch_mu);
+    auto it = d3::tma::g_batches.find(desc);
+    HL_CHECK_ARG(it != d3::tma::g_batches.end() && it->second.first == n_domains && it->second.second == n_items,
+                 "d3q27 batch: descriptors not prepared for %d domains and %d items", n_domains, n_items);
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const auto* doms = static_cast<const d3::tma::BatchDomain*>(desc);
+  switch (storage->dtype) {
+    case HL_F32: return d3::tma::launch_batch<StoreF32, 4>(doms, n_domains, n_items, vis_shear, *storage, parity, status, st);
+    case HL_F16: return d3::tma::launch_batch<StoreF16, 4>(doms, n_domains, n_items, vis_shear, *storage, parity, status, st);
+    case HL_BF16: return d3::tma::launch_batch<StoreBF16, 4>(doms, n_domains, n_items, vis_shear, *storage, parity, status, st);
+    default: break;
+  }
+  set_error("d3q27 batch: storage dtype %d not supported", int(storage->dtype));
+  return HL_ERR_UNSUPPORTED;
+}

@@ -83,7 +83,8 @@ def _image3d(flow, mode: int, axis: int, index: int, kind: int, thickness: float
     name, shape = _PLANE[axis]
     out = _buffer(flow, name, shape(flow))
     s = None
-    solver = getattr(flow, "solver", None)
+    ref = getattr(flow, "solver_ref", None)
+    solver = ref() if ref is not None else None
     if solids and solver is not None and solver.has_meshes:
         s = solver._solids_struct(flow.world_index)
     _lib.check(_lib.lib().hl_d3q27_image(flow.world_struct(), mode, axis, int(index), kind, float(flow.grid_length), s,

@@ -10,6 +10,7 @@ change (the reference invalidates its graph the same way, karman_lbm_env_3d.py:2
 """
 from __future__ import annotations
 
+import weakref
 from typing import Any, Dict, Optional, Sequence, Tuple
 
 import numpy as np
@@ -86,8 +87,10 @@ class LBM_Solver3D:
             f.Initialize(nx, ny, nz, n_objects=solid_num, device=self.device, storage=storage,
                          u_scale=u_scale, s_scale=s_scale, periodic=periodic, with_flag=with_flag,
                          with_force=with_force)
-            # the solver holds the meshes; the field diagnostics find them from the world
-            f.solver, f.world_index = self, k
+            # the solver holds the meshes; the field diagnostics find them from the world (a
+            # weak reference: a solver <-> world cycle would leave the solver, and the CUDA
+            # graphs it holds, to the cyclic garbage collector, which may run during a capture)
+            f.solver_ref, f.world_index = weakref.ref(self), k
             self.flows.append(f)
         stream = _lib.stream_ptr()
         L = _lib.lib()
@@ -186,9 +189,12 @@ class LBM_Solver3D:
         return any(t is not None and len(t) for t in self._mesh_tris)
 
     # ------------------------------------------------------------------ stepping
-    def _launch(self, parity: int, stream, loads_out=None) -> None:
+    def _launch(self, parity: int, stream, loads_out=None, stream_collide: bool = True) -> None:
         """One step of every world on ``stream``. ``loads_out`` (optional, per world a pair of
-        device pointers) redirects the binary32 solid force / torque [n][3] of the step."""
+        device pointers) redirects the binary32 solid force / torque [n][3] of the step.
+        ``stream_collide=False`` leaves out the stream-collide launch (a batched launch over
+        several solvers' worlds, hl_d3q27_stream_collide_batch, does it) and enqueues only the
+        cut links and the boundaries that follow it."""
         L = _lib.lib()
         meshes = self.has_meshes
         for k, f in enumerate(self.flows):
@@ -197,7 +203,8 @@ class LBM_Solver3D:
             if self.diagnostics:
                 diag = _lib.hl_diag(self._diag_scratch[k].data_ptr(), self._diag_scratch[k].numel(),
                                     self.mass[k:k + 1].data_ptr(), self.health[k:k + 1].data_ptr())
-            _lib.check(L.hl_d3q27_stream_collide(w, float(f.vis_shear), diag, stream), "stream_and_collide_3d")
+            if stream_collide:
+                _lib.check(L.hl_d3q27_stream_collide(w, float(f.vis_shear), diag, stream), "stream_and_collide_3d")
             if meshes:
                 sst = self._solids_struct(k)
                 if loads_out is not None:

@@ -6,13 +6,20 @@ control step (``substeps`` LBM steps), for ``control_steps`` control steps.
 
 ``ServeEngine`` runs requests with continuous batching: a request that has arrived is admitted
 as soon as a slot is free and its fields fit the HBM budget; its fields stay on the device for
-its whole life; every active request advances one control step per tick, each on its own CUDA
-stream, so the domains' kernels overlap on the device (the small domains fill the SMs the big
-ones leave idle). A domain's control step (pose updates, stream-collide, cut links, boundaries
-and load copies for all substeps) is captured once into a CUDA graph at admission, so a tick
-is one graph launch per domain, and the poses of every domain's next control step are computed
-on the host while the tick runs on the device. Admission (allocation, initial state, graph
-capture) happens between ticks and counts in the wall time, not in a control step's latency.
+its whole life; every active request advances one control step per tick. By default a
+domain's whole control step (pose updates, stream-collide, cut links, boundaries and load
+copies for all substeps) is captured once into a CUDA graph at admission and each tick
+launches every active domain's graph on its own CUDA stream, so the domains' kernels overlap
+on the device. With ``batched=True`` each substep is instead ONE stream-collide launch over
+every active domain (hl_d3q27_stream_collide_batch: the tiles of all domains share the SMs),
+then each domain's cut links, boundaries, load copy and next pose on its own stream; once the
+set of active domains has held for two ticks, the whole control step of the set is one CUDA
+graph (``TickGraph``). Both give the same results; the batched form's stream-collide is
+faster, but its cut links and boundaries then run between two batched launches instead of
+behind other domains' stream-collides, and on B200 the two forms measure within a few
+percent of each other. The poses of every domain's next control step are computed on the host
+while the tick runs on the device. Admission (allocation, initial state, graph capture)
+happens between ticks and counts in the wall time, not in a control step's latency.
 ``run_plain`` is the baseline: the same requests one at a time through the plain drop-in
 solver (LBM_Solver3D, float32 storage), one graph launch per LBM step.
 
@@ -21,11 +28,13 @@ read and write only that domain's buffers.
 """
 from __future__ import annotations
 
+import contextlib
+import gc
 import math
 import os
 import time
 from dataclasses import dataclass, field
-from typing import Dict, List, Optional, Tuple
+from typing import Dict, List, Tuple
 
 import numpy as np
 import torch
@@ -33,11 +42,26 @@ import torch
 from . import _lib
 from .lbm3d import LBM_Solver3D
 
+import ctypes
+
 SEGMENTS = 5
 # One hardware work queue per domain stream: with CUDA's default of 8, the streams of more
 # than 8 domains share queues and their graphs run one after another. Effective only when
 # this module is imported before the process creates its CUDA context.
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
+
+@contextlib.contextmanager
+def _capturing():
+    """No cyclic garbage collection while a CUDA graph is captured: a collected object that
+    owns a CUDA graph would destroy it mid-capture, which invalidates the capture."""
+    enabled = gc.isenabled()
+    gc.disable()
+    try:
+        yield
+    finally:
+        if enabled:
+            gc.enable()
 
 
 # ----------------------------------------------------------------------------- bodies
@@ -146,9 +170,14 @@ def domain_bytes(side: int, storage: str) -> int:
 # ----------------------------------------------------------------------------- one domain
 class Domain:
     """A resident request: its solver (one world), swimmer, pose and load buffers, stream and
-    the CUDA graph of one control step."""
+    the CUDA graphs of its work (``batched``: the pose update of substep 0 and, per substep k,
+    what follows the batched stream-collide; otherwise one graph of the whole control step)."""
 
-    def __init__(self, req: Request, storage: str, vis: float, device, use_graph: bool = True):
+    def __init__(self, req: Request, storage: str, vis: float, device, use_graph: bool = True,
+                 batched: bool = False):
+        if req.substeps < 2 or req.substeps % 2:
+            # every control step starts from buffer 0: an even number of substeps ends there
+            raise ValueError(f"request {req.rid}: substeps must be even and positive, got {req.substeps}")
         self.req = req
         self.device = device
         self.stream = torch.cuda.Stream(device=device)
@@ -180,29 +209,55 @@ class Domain:
             self.ids = torch.arange(SEGMENTS, dtype=torch.int32, device=dev)
             self.zeros3 = torch.zeros((SEGMENTS, 3), dtype=torch.float32, device=dev)
             self.ones = torch.ones(SEGMENTS, dtype=torch.float32, device=dev)
+        self.batched = bool(batched)
         self.graph = None
+        self.pre_graph = None
+        self.post_graphs: List[torch.cuda.CUDAGraph] = []
         if use_graph:
             self.stream.synchronize()
-            self.graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(self.graph, stream=self.stream):
-                self._control_step()
+            if self.batched:
+                self.pre_graph = self._capture(lambda: self._pose(0))
+                S = req.substeps
+                self.post_graphs = [self._capture(lambda k=k: self._after_stream_collide(k, k + 1 < S))
+                                    for k in range(S)]
+            else:
+                self.graph = self._capture(self._control_step)
         self.event = torch.cuda.Event()
+        self.ready = torch.cuda.Event()  # batched: the domain's part of the current substep is done
+
+    def _capture(self, fn) -> torch.cuda.CUDAGraph:
+        g = torch.cuda.CUDAGraph()
+        with _capturing(), torch.cuda.graph(g, stream=self.stream):
+            fn()
+        return g
+
+    def _pose(self, k: int) -> None:
+        """The swimmer's pose of substep k from the pose buffer (convert_and_update_solid_batch_3d)."""
+        s = self.solver
+        _lib.check(_lib.lib().hl_couple3d_update_solids(
+            1, SEGMENTS, SEGMENTS, _lib.ptr(self.ids), self.pos_dev[k].data_ptr(), self.quat_dev[k].data_ptr(),
+            _lib.ptr(self.zeros3), _lib.ptr(self.zeros3), _lib.ptr(self.ones),
+            _lib.ptr(s.solid_position_all), _lib.ptr(s.solid_quaternion_all), _lib.ptr(s.mesh_transforms_all),
+            _lib.ptr(s.mesh_transforms_last_all), _lib.ptr(s.mesh_transforms_initialized_all), _lib.stream_ptr()),
+            "pose update")
+
+    def _loads_out(self, k: int):
+        return [(self.loads_dev[k, 0].data_ptr(), self.loads_dev[k, 1].data_ptr())]
+
+    def _after_stream_collide(self, k: int, next_pose: bool) -> None:
+        """Substep k after its stream-collide: cut links (loads into slot k), boundaries, and the
+        pose of substep k + 1."""
+        self.solver._launch(k % 2, _lib.stream_ptr(), loads_out=self._loads_out(k), stream_collide=False)
+        if next_pose:
+            self._pose(k + 1)
 
     def _control_step(self) -> None:
-        """One control step on the current stream: per substep, the swimmer's pose from the
-        pose buffer (convert_and_update_solid_batch_3d) and one LBM step with the cut links,
-        whose loads go straight to the substep's slot of the load buffer."""
-        s = self.solver
-        L = _lib.lib()
-        st = _lib.stream_ptr()
+        """One control step on the current stream: per substep, the swimmer's pose and one LBM
+        step with the cut links, whose loads go straight to the substep's slot of the load
+        buffer."""
         for k in range(self.req.substeps):
-            _lib.check(L.hl_couple3d_update_solids(
-                1, SEGMENTS, SEGMENTS, _lib.ptr(self.ids), self.pos_dev[k].data_ptr(), self.quat_dev[k].data_ptr(),
-                _lib.ptr(self.zeros3), _lib.ptr(self.zeros3), _lib.ptr(self.ones),
-                _lib.ptr(s.solid_position_all), _lib.ptr(s.solid_quaternion_all), _lib.ptr(s.mesh_transforms_all),
-                _lib.ptr(s.mesh_transforms_last_all), _lib.ptr(s.mesh_transforms_initialized_all), st),
-                "pose update")
-            s._launch(k % 2, st, loads_out=[(self.loads_dev[k, 0].data_ptr(), self.loads_dev[k, 1].data_ptr())])
+            self._pose(k)
+            self.solver._launch(k % 2, _lib.stream_ptr(), loads_out=self._loads_out(k))
 
     def stage_poses(self, step: int) -> None:
         """Host: the swimmer's poses for every substep of control step ``step``, into the host
@@ -227,6 +282,30 @@ class Domain:
             self.loads_host.copy_(self.loads_dev, non_blocking=True)
             self.event.record(self.stream)
 
+    # batched: the engine interleaves these with the batched stream-collide of each substep
+    def begin(self) -> None:
+        """Pose upload and the pose of substep 0; records ``ready``."""
+        buf = self.done % 2
+        with torch.cuda.stream(self.stream):
+            self.pos_dev.copy_(self.pos_host[buf], non_blocking=True)
+            self.quat_dev.copy_(self.quat_host[buf], non_blocking=True)
+            self.pre_graph.replay()
+            self.ready.record(self.stream)
+
+    def after(self, k: int, stream_collide_done: torch.cuda.Event) -> None:
+        """Substep k's part after the batched stream-collide (which ``stream_collide_done``
+        marks); records ``ready``."""
+        self.stream.wait_event(stream_collide_done)
+        with torch.cuda.stream(self.stream):
+            self.post_graphs[k].replay()
+            self.ready.record(self.stream)
+
+    def end(self) -> None:
+        """The load download; records ``event``."""
+        with torch.cuda.stream(self.stream):
+            self.loads_host.copy_(self.loads_dev, non_blocking=True)
+            self.event.record(self.stream)
+
     def finish(self, latency: float) -> None:
         # per substep and segment: force then torque (the plain baseline's layout)
         self.loads.append(np.concatenate([self.loads_host[:, 0].numpy(), self.loads_host[:, 1].numpy()], axis=2))
@@ -239,7 +318,78 @@ class Domain:
 
     def release(self) -> None:
         self.graph = None
+        self.pre_graph = None
+        self.post_graphs = []
         self.solver = None
+
+
+class BatchStep:
+    """The batched stream-collide of a set of domains (hl_d3q27_stream_collide_batch): the
+    descriptors (buffers, sizes, tensor maps of every domain) are written once for the set;
+    each substep is then one launch at that substep's parity."""
+
+    def __init__(self, domains: List["Domain"], stream: torch.cuda.Stream):
+        L = _lib.lib()
+        if len({d.req.substeps for d in domains}) != 1:
+            raise ValueError("batched stream-collide: the domains need one number of substeps")
+        flows = [d.solver.flows[0] for d in domains]
+        vis = {float(f.vis_shear) for f in flows}
+        if len(vis) != 1:
+            raise ValueError("batched stream-collide: the domains need one viscosity")
+        self.vis = vis.pop()
+        self.n = len(flows)
+        worlds = (_lib.hl_world3d * self.n)(*[f.world_struct(0) for f in flows])
+        self.storage = worlds[0].storage
+        nbytes = int(L.hl_d3q27_batch_bytes(self.n))
+        dev = flows[0].device
+        self.buf = torch.empty(nbytes + 64, dtype=torch.uint8, device=dev)
+        self.ptr = (self.buf.data_ptr() + 63) // 64 * 64
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        n_items = ctypes.c_int(0)
+        _lib.check(L.hl_d3q27_batch_prepare(worlds, self.n, self.ptr, nbytes, ctypes.byref(n_items),
+                                            _lib.stream_ptr(stream)), "batched stream-collide (prepare)")
+        self.n_items = int(n_items.value)
+
+    def launch(self, parity: int, stream: torch.cuda.Stream) -> None:
+        _lib.check(_lib.lib().hl_d3q27_stream_collide_batch(
+            self.ptr, self.n, self.n_items, self.vis, ctypes.byref(self.storage), int(parity),
+            self.status.data_ptr(), _lib.stream_ptr(stream)), "batched stream-collide")
+
+
+class TickGraph:
+    """One control step of a fixed set of batched domains as ONE CUDA graph: the pose of
+    substep 0 of every domain, then per substep the batched stream-collide followed by every
+    domain's cut links, boundaries, load copy and next pose, each domain on its own branch.
+    Replaying it costs the host one launch instead of a few calls per domain and substep (which
+    leave the device idle between substeps). The pose upload and load download stay outside, on
+    the replaying stream."""
+
+    def __init__(self, domains: List[Domain], batch: "BatchStep", main: torch.cuda.Stream):
+        S = domains[0].req.substeps
+        torch.cuda.synchronize()
+        fork = torch.cuda.Event()
+        sc_done = [torch.cuda.Event() for _ in range(S)]
+        ready = [[torch.cuda.Event() for _ in range(S + 1)] for _ in domains]
+        self.graph = torch.cuda.CUDAGraph()
+        with _capturing(), torch.cuda.graph(self.graph, stream=main):
+            fork.record(main)
+            for d, rd in zip(domains, ready):
+                d.stream.wait_event(fork)
+                with torch.cuda.stream(d.stream):
+                    d._pose(0)
+                rd[0].record(d.stream)
+            for k in range(S):
+                for rd in ready:
+                    main.wait_event(rd[k])
+                batch.launch(k % 2, main)
+                sc_done[k].record(main)
+                for d, rd in zip(domains, ready):
+                    d.stream.wait_event(sc_done[k])
+                    with torch.cuda.stream(d.stream):
+                        d._after_stream_collide(k, k + 1 < S)
+                    rd[k + 1].record(d.stream)
+            for rd in ready:
+                main.wait_event(rd[S])
 
 
 # ----------------------------------------------------------------------------- engines
@@ -265,13 +415,16 @@ class ServeEngine:
     """Continuous batching of resident domains (see the module docstring)."""
 
     def __init__(self, storage: str = "float16", budget_bytes: float = 150e9, max_active: int = 32,
-                 vis: float = 0.01, device=None, keep_fields: bool = False):
+                 vis: float = 0.01, device=None, keep_fields: bool = False, batched: bool = False):
         self.storage = storage
         self.budget = float(budget_bytes)
         self.max_active = int(max_active)
         self.vis = float(vis)
         self.device = _lib.require_cuda(device)
         self.keep_fields = bool(keep_fields)
+        # per-domain graphs unless asked (see the module docstring); the batched stream-collide
+        # takes float32/16 and bfloat16 storage only
+        self.batched = bool(batched) and storage != "float64"
 
     def run(self, requests: List[Request], realtime: bool = True) -> ServeStats:
         """Serve the requests (arrival times honoured when ``realtime``) until all finish."""
@@ -293,12 +446,16 @@ class ServeEngine:
                 if used + need > self.budget:
                     break
                 r = pending.pop(0)
-                d = Domain(r, self.storage, self.vis, self.device)
+                d = Domain(r, self.storage, self.vis, self.device, batched=self.batched)
                 d.stage_poses(0)
                 active.append(d)
                 used += need
                 order.append(r.rid)
 
+        main = torch.cuda.Stream(device=self.device)
+        sc_done = torch.cuda.Event()
+        tick_done = torch.cuda.Event()
+        batch, batch_ids, tick_graph, stable = None, None, None, 0
         while pending or active:
             admit()
             if not active:
@@ -306,15 +463,52 @@ class ServeEngine:
                 continue
             peak = max(peak, len(active))
             running = list(active)
+            if self.batched:
+                if batch_ids != [id(d) for d in running]:
+                    batch = BatchStep(running, main)  # the set changed: new descriptors
+                    batch_ids = [id(d) for d in running]
+                    tick_graph, stable = None, 0
+                else:
+                    stable += 1
+                # one graph per set, once the set has held for two ticks (while domains arrive
+                # or finish every tick, capturing would cost more than it saves)
+                if tick_graph is None and stable >= 2:
+                    tick_graph = TickGraph(running, batch, main)
             t0 = time.perf_counter()
-            for d in running:
-                d.launch()
+            if tick_graph is not None:
+                with torch.cuda.stream(main):
+                    for d in running:
+                        buf = d.done % 2
+                        d.pos_dev.copy_(d.pos_host[buf], non_blocking=True)
+                        d.quat_dev.copy_(d.quat_host[buf], non_blocking=True)
+                    tick_graph.graph.replay()
+                    for d in running:
+                        d.loads_host.copy_(d.loads_dev, non_blocking=True)
+                    tick_done.record(main)
+            elif self.batched:
+                for d in running:
+                    d.begin()
+                for k in range(running[0].req.substeps):
+                    for d in running:
+                        main.wait_event(d.ready)
+                    batch.launch(k % 2, main)
+                    sc_done.record(main)
+                    for d in running:
+                        d.after(k, sc_done)
+                for d in running:
+                    d.end()
+            else:
+                for d in running:
+                    d.launch()
             # while the device works: the poses of every domain's next control step
             for d in running:
                 if d.done + 1 < d.req.control_steps:
                     d.stage_poses(d.done + 1)
-            for d in running:
-                d.event.synchronize()
+            if tick_graph is not None:
+                tick_done.synchronize()
+            else:
+                for d in running:
+                    d.event.synchronize()
             t1 = time.perf_counter()
             for d in running:
                 d.finish(t1 - t0)
