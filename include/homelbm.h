@@ -417,6 +417,24 @@ HL_API int hl_d2q9_image(const hl_world2d* w, int kind, float param, float grid_
 HL_API int hl_d3q27_image(const hl_world3d* w, int mode, int axis, int index, int kind, float grid_length,
                           const hl_solids3d* solids, float thickness, float* out, hl_stream stream);
 
+/* The live view's slice stack (tools/lbm3d_realtime_control.py:68-148, 157-182; a device
+ * RGBA buffer replaces the GL atlas):
+ *  - hl_d3q27_live_slices: values[(slice * plane_height + q) * plane_width + p] is the
+ *    vorticity component color_axis (0 x, 1 y, 2 z) at the cell of plane p, q of slice
+ *    slice_positions[slice] along slice_axis, the in-plane coordinates p * stride and
+ *    q * stride clamped to the grid; central differences clamped at the border, divided by the
+ *    clamped span; zero within boundary_margin of a face. With collect_histogram, every
+ *    |value| > 1e-8 adds one to histogram[bin], bin = floor(256 * clamp((log|value| - log 1e-8)
+ *    / -log 1e-8, 0, 0.999999)) (the caller zeroes the 256 int32 bins first). slice_positions
+ *    is device memory; a position outside the grid gives zeros and no count.
+ *  - hl_live_rgba: rgba[4 i ..] = the blue-white-red map of values[i] / vmax (clamped) and
+ *    255 alpha (clamped to [0, 1]), each channel truncated to a byte.
+ * Stream-ordered, allocation-free, capturable. */
+HL_API int hl_d3q27_live_slices(const hl_world3d* w, const int32_t* slice_positions, int n_slices, int plane_width,
+                                int plane_height, int stride, int slice_axis, int color_axis, int boundary_margin,
+                                int collect_histogram, float* values, int32_t* histogram, hl_stream stream);
+HL_API int hl_live_rgba(const float* values, long long n, float vmax, float alpha, uint8_t* rgba, hl_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -7,7 +7,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int, c_int32, c_size_t,
+from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int, c_int32, c_longlong, c_size_t,
                     c_void_p)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -83,6 +83,9 @@ _SIGS = {
     "hl_d3q27_apply_bc": ([POINTER(hl_world3d), POINTER(hl_bc3d), c_void_p, c_void_p], c_int),
     "hl_d3q27_scratch_bytes": ([POINTER(hl_world3d)], c_size_t),
     "hl_d3q27_stream_collide_noalloc": ([POINTER(hl_world3d), c_double, c_void_p, c_void_p, c_void_p], c_int),
+    "hl_d3q27_live_slices": ([POINTER(hl_world3d), c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int,
+                              c_void_p, c_void_p, c_void_p], c_int),
+    "hl_live_rgba": ([c_void_p, c_longlong, c_float, c_float, c_void_p, c_void_p], c_int),
     "hl_d3q27_batch_bytes": ([c_int], c_size_t),
     "hl_d3q27_batch_prepare": ([POINTER(hl_world3d), c_int, c_void_p, c_size_t, POINTER(c_int), c_void_p], c_int),
     "hl_d3q27_stream_collide_batch": ([c_void_p, c_int, c_int, c_double, POINTER(hl_storage), c_int, c_void_p,

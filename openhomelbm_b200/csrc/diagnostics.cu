@@ -7,6 +7,9 @@
 //   3D (envs/lbm3d/lbm_func_3d.py): get_u_img_xy_3d / _yz_3d 753-776, get_vorticity_xy_3d /
 //      _yz_3d 779-840, the _with_solid_3d variants 843-987, the projections 990-1313 with
 //      any_mesh_hit_along_ray_3d 320-362.
+//   live view (tools/lbm3d_realtime_control.py): _extract_live_vorticity_slices 68-148 with
+//      its log-magnitude histogram, _live_vorticity_to_rgba 157-182 (into a device RGBA buffer
+//      instead of the GL atlas).
 // Velocities are the decoded u of the current buffer, in binary32 as the reference's fields.
 //
 // Third-party queries of the reference, restated: wp.mesh_query_ray (any hit with
@@ -392,6 +395,96 @@ template <class S> __global__ void __launch_bounds__(BLOCK) image3d_kernel(const
   a.out[i] = a.solids && any_mesh_hit(a.s, origin, dir, max_t) ? SOLID_MARK : best;
 }
 
+// ------------------------------------------------------------------------------- live view
+constexpr int LIVE_BINS = 256;
+constexpr float LIVE_LOG_MIN = -18.420680743952367f;  // log(1e-8)
+constexpr float LIVE_LOG_MAX = 0.0f;                   // log(1)
+
+struct ArgsLive {
+  W3 w;
+  const int32_t* slice_pos;
+  int n_slices, width, height, stride, slice_axis, color_axis, margin, collect;
+  float* values;
+  int32_t* hist;
+};
+
+// One sample of a stack of planes (p, q, slice) sampled every `stride` cells: a vorticity
+// component from central differences clamped at the border (divided by the clamped span),
+// zero within `margin` of a face; |value| > 1e-8 counts in the bin of its log magnitude over
+// [log 1e-8, log 1]. A slice position outside the grid gives zeros and no count.
+template <class S> __global__ void __launch_bounds__(BLOCK) live_slices_kernel(const __grid_constant__ ArgsLive a) {
+  const long long per = (long long)a.width * a.height;
+  const long long i = (long long)blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= per * a.n_slices) return;
+  const int slice = int(i / per);
+  const int rem = int(i - (long long)slice * per);
+  const int q = rem / a.width, p = rem - q * a.width;
+  const int nx = a.w.n[0], ny = a.w.n[1], nz = a.w.n[2];
+  const int pos = a.slice_pos[slice];
+  const int along = a.slice_axis == 0 ? nx : a.slice_axis == 1 ? ny : nz;
+  if (pos < 0 || pos >= along) {
+    a.values[i] = 0.f;
+    return;
+  }
+  int x, y, z;
+  if (a.slice_axis == 0) {
+    x = pos, y = min(p * a.stride, ny - 1), z = min(q * a.stride, nz - 1);
+  } else if (a.slice_axis == 1) {
+    x = min(p * a.stride, nx - 1), y = pos, z = min(q * a.stride, nz - 1);
+  } else {
+    x = min(p * a.stride, nx - 1), y = min(q * a.stride, ny - 1), z = pos;
+  }
+  const int xm = max(x - 1, 0), xp = min(x + 1, nx - 1);
+  const int ym = max(y - 1, 0), yp = min(y + 1, ny - 1);
+  const int zm = max(z - 1, 0), zp = min(z + 1, nz - 1);
+  const float inv_dx = 1.f / float(max(xp - xm, 1));
+  const float inv_dy = 1.f / float(max(yp - ym, 1));
+  const float inv_dz = 1.f / float(max(zp - zm, 1));
+  auto u = [&](int cx, int cy, int cz, int comp) {
+    const int c[3] = {cx, cy, cz};
+    return u3<S>(a.w, c, comp);
+  };
+  float value;
+  if (a.color_axis == 0)
+    value = (u(x, yp, z, 2) - u(x, ym, z, 2)) * inv_dy - (u(x, y, zp, 1) - u(x, y, zm, 1)) * inv_dz;
+  else if (a.color_axis == 1)
+    value = (u(x, y, zp, 0) - u(x, y, zm, 0)) * inv_dz - (u(xp, y, z, 2) - u(xm, y, z, 2)) * inv_dx;
+  else
+    value = (u(xp, y, z, 1) - u(xm, y, z, 1)) * inv_dx - (u(x, yp, z, 0) - u(x, ym, z, 0)) * inv_dy;
+  if (x < a.margin || x >= nx - a.margin || y < a.margin || y >= ny - a.margin || z < a.margin ||
+      z >= nz - a.margin)
+    value = 0.f;
+  a.values[i] = value;
+  if (a.collect) {
+    const float mag = fabsf(value);
+    if (mag > 1.0e-8f) {
+      const float normalized = (logf(mag) - LIVE_LOG_MIN) / (LIVE_LOG_MAX - LIVE_LOG_MIN);
+      const int bin = int(fminf(fmaxf(normalized, 0.f), 0.999999f) * float(LIVE_BINS));
+      atomicAdd(&a.hist[bin], 1);
+    }
+  }
+}
+
+// Blue-white-red map of value / vmax (clamped to [-1, 1]) to RGBA bytes, alpha the same for
+// every pixel; a channel is the binary32 level truncated to an integer.
+__global__ void __launch_bounds__(BLOCK) live_rgba_kernel(const float* values, uint8_t* rgba, long long n, float vmax,
+                                                          float alpha) {
+  const long long i = (long long)blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= n) return;
+  const float normalized = fminf(fmaxf(0.5f + 0.5f * values[i] / fmaxf(vmax, 1.0e-8f), 0.f), 1.f);
+  float r, g, b;
+  if (normalized < 0.5f) {
+    const float t = normalized * 2.f;
+    r = 255.f * t, g = 255.f * t, b = 255.f;
+  } else {
+    const float t = (normalized - 0.5f) * 2.f;
+    r = 255.f, g = 255.f * (1.f - t), b = 255.f * (1.f - t);
+  }
+  uint8_t* px = rgba + 4 * i;
+  px[0] = uint8_t(r), px[1] = uint8_t(g), px[2] = uint8_t(b);
+  px[3] = uint8_t(255.f * fminf(fmaxf(alpha, 0.f), 1.f));
+}
+
 template <class S, class A, class K> int launch(K kern, const A& a, long long pixels, cudaStream_t st) {
   if (pixels == 0) return HL_OK;
   kern<<<unsigned((pixels + BLOCK - 1) / BLOCK), BLOCK, 0, st>>>(a);
@@ -472,4 +565,52 @@ extern "C" int hl_d3q27_image(const hl_world3d* w, int mode, int axis, int index
   }
   set_error("image: storage dtype %d not supported", int(w->storage.dtype));
   return HL_ERR_UNSUPPORTED;
+}
+
+extern "C" int hl_d3q27_live_slices(const hl_world3d* w, const int32_t* slice_positions, int n_slices, int plane_width,
+                                    int plane_height, int stride, int slice_axis, int color_axis, int boundary_margin,
+                                    int collect_histogram, float* values, int32_t* histogram, hl_stream stream) {
+  HL_CHECK_ARG(w != nullptr && w->cur != nullptr && values != nullptr && slice_positions != nullptr,
+               "live slices: world, cur, slice positions or values is NULL");
+  HL_CHECK_ARG(w->nx >= 1 && w->ny >= 1 && w->nz >= 1, "live slices: bad grid");
+  HL_CHECK_ARG(n_slices >= 1 && plane_width >= 1 && plane_height >= 1 && stride >= 1,
+               "live slices: %d slices of %d x %d, stride %d", n_slices, plane_width, plane_height, stride);
+  HL_CHECK_ARG((long long)n_slices * plane_width * plane_height < (1ll << 38), "live slices: too many samples");
+  HL_CHECK_ARG(slice_axis >= 0 && slice_axis <= 2 && color_axis >= 0 && color_axis <= 2,
+               "live slices: slice axis %d, colour axis %d", slice_axis, color_axis);
+  HL_CHECK_ARG(boundary_margin >= 0, "live slices: negative margin");
+  HL_CHECK_ARG(!collect_histogram || histogram != nullptr, "live slices: the histogram is NULL");
+  diag::ArgsLive a{};
+  a.w = {{w->nx, w->ny, w->nz}, w->cur, nullptr, w->storage.u_scale > 0.f ? w->storage.u_scale : 1.f};
+  a.slice_pos = slice_positions;
+  a.n_slices = n_slices;
+  a.width = plane_width;
+  a.height = plane_height;
+  a.stride = stride;
+  a.slice_axis = slice_axis;
+  a.color_axis = color_axis;
+  a.margin = boundary_margin;
+  a.collect = collect_histogram != 0;
+  a.values = values;
+  a.hist = histogram;
+  const long long n = (long long)n_slices * plane_width * plane_height;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  switch (w->storage.dtype) {
+    case HL_F32: return diag::launch<StoreF32>(diag::live_slices_kernel<StoreF32>, a, n, st);
+    case HL_F16: return diag::launch<StoreF16>(diag::live_slices_kernel<StoreF16>, a, n, st);
+    case HL_BF16: return diag::launch<StoreBF16>(diag::live_slices_kernel<StoreBF16>, a, n, st);
+    case HL_F64: return diag::launch<StoreF64>(diag::live_slices_kernel<StoreF64>, a, n, st);
+  }
+  set_error("live slices: storage dtype %d not supported", int(w->storage.dtype));
+  return HL_ERR_UNSUPPORTED;
+}
+
+extern "C" int hl_live_rgba(const float* values, long long n, float vmax, float alpha, uint8_t* rgba, hl_stream stream) {
+  HL_CHECK_ARG(n >= 0 && (n == 0 || (values != nullptr && rgba != nullptr)), "live rgba: values or rgba is NULL");
+  if (n == 0) return HL_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  diag::live_rgba_kernel<<<unsigned((n + diag::BLOCK - 1) / diag::BLOCK), diag::BLOCK, 0, st>>>(values, rgba, n, vmax,
+                                                                                                 alpha);
+  HL_LAUNCH_CHECK("live rgba");
+  return HL_OK;
 }

@@ -155,3 +155,67 @@ def get_vorticity_projection_side_3d(flow) -> torch.Tensor:
 def get_vorticity_projection_front_3d(flow) -> torch.Tensor:
     """y vorticity of largest magnitude along y into flow.u_img_xz_front (1260-1313)."""
     return _image3d(flow, 1, 1, 0, 2, solids=True)
+
+
+# ----------------------------------------------------------------------------- live view
+# The slice stack of the reference's live 3D view (tools/lbm3d_realtime_control.py:58-182,
+# 820-869), on device buffers instead of a GL atlas.
+_LIVE_HISTOGRAM_BINS = 256
+_LIVE_LOG_VORT_MIN = -18.420680743952367  # log(1e-8)
+_LIVE_LOG_VORT_MAX = 0.0                  # log(1.0)
+
+
+def clear_live_histogram(histogram: torch.Tensor) -> None:
+    """_clear_live_histogram: zero the 256 int32 bins."""
+    histogram.zero_()
+
+
+def extract_live_vorticity_slices(flow, slice_positions: torch.Tensor, values: torch.Tensor,
+                                  histogram: torch.Tensor, plane_width: int, plane_height: int, stride: int,
+                                  slice_axis: int, color_axis: int, boundary_margin: int,
+                                  collect_histogram: int) -> None:
+    """_extract_live_vorticity_slices (68-148): signed vorticity component `color_axis` on a
+    stack of planes normal to `slice_axis` at `slice_positions` (int32, device), sampled every
+    `stride` cells, into values[(slice * plane_height + q) * plane_width + p] (float32); with
+    `collect_histogram`, the log-magnitude histogram of the nonzero values is added to
+    `histogram` (int32, 256 bins)."""
+    n = int(slice_positions.numel())
+    for t, dt, need in ((slice_positions, torch.int32, n), (values, torch.float32, n * plane_width * plane_height),
+                        (histogram, torch.int32, _LIVE_HISTOGRAM_BINS)):
+        if t.dtype != dt or not t.is_cuda or not t.is_contiguous() or t.numel() < need:
+            raise ValueError("live slices: slice_positions int32 (n), values float32 (n * width * height) and "
+                             "histogram int32 (256), contiguous CUDA tensors")
+    _lib.check(_lib.lib().hl_d3q27_live_slices(
+        flow.world_struct(), slice_positions.data_ptr(), n, int(plane_width), int(plane_height), int(stride),
+        int(slice_axis), int(color_axis), int(boundary_margin), int(collect_histogram), values.data_ptr(),
+        histogram.data_ptr(), _lib.stream_ptr()), "live slices")
+
+
+def live_vorticity_to_rgba(values: torch.Tensor, rgba: torch.Tensor, vmax: float, alpha: float) -> None:
+    """_live_vorticity_to_rgba (157-182): blue-white-red map of values / vmax into rgba (uint8,
+    4 per value)."""
+    if values.dtype != torch.float32 or rgba.dtype != torch.uint8 or rgba.numel() < 4 * values.numel() \
+            or not (values.is_cuda and rgba.is_cuda and values.is_contiguous() and rgba.is_contiguous()):
+        raise ValueError("live rgba: values float32 and rgba uint8 (4 per value), contiguous CUDA tensors")
+    _lib.check(_lib.lib().hl_live_rgba(values.data_ptr(), values.numel(), float(vmax), float(alpha), rgba.data_ptr(),
+                                       _lib.stream_ptr()), "live rgba")
+
+
+def vmax_from_histogram(counts, percentile: float, previous=None) -> float:
+    """_update_vmax_from_histogram (820-831): the centre of the bin holding the `percentile`-th
+    count, mapped back from log magnitude; 1e-6 for an empty histogram; against a previous
+    value, the larger of it decayed by 0.96 and the new one (at least 1e-8). Host side."""
+    import math
+
+    import numpy as np
+
+    counts = np.asarray(counts).astype(np.int64, copy=False)
+    total = int(counts.sum())
+    if total <= 0:
+        current = 1.0e-6
+    else:
+        target = max(1, int(math.ceil(total * float(percentile) / 100.0)))
+        bin_id = int(np.searchsorted(np.cumsum(counts), target, side="left"))
+        fraction = (min(bin_id, _LIVE_HISTOGRAM_BINS - 1) + 0.5) / _LIVE_HISTOGRAM_BINS
+        current = math.exp(_LIVE_LOG_VORT_MIN + fraction * (_LIVE_LOG_VORT_MAX - _LIVE_LOG_VORT_MIN))
+    return max(current, 1.0e-8) if previous is None else max(previous * 0.96, current, 1.0e-8)

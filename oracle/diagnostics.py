@@ -7,6 +7,8 @@ Every function works in binary32 in the reference's operation order:
       get_solid_boundary_img 804-866;
   3D, envs/lbm3d/lbm_func_3d.py: slices 753-840, solid overlays 843-987, projections 990-1313,
       any_mesh_hit_along_ray_3d 320-362.
+  live view, tools/lbm3d_realtime_control.py: _extract_live_vorticity_slices 68-148,
+      _live_vorticity_to_rgba 157-182.
 The reference's mesh queries live in NVIDIA Warp (wp.mesh_query_ray,
 wp.mesh_query_point_sign_normal), not in the reference tree; they are restated as a
 Moller-Trumbore any-hit test and as the closest point (Ericson, Real-Time Collision Detection,
@@ -289,3 +291,75 @@ def solid_plane_mask(shape, axis, index, tri_offset, tris, transforms, scale_siz
                     out[i, j] = True
                     break
     return out
+
+
+# ------------------------------------------------------------------------------ live view
+LIVE_BINS = 256
+LIVE_LOG_MIN = F(-18.420680743952367)  # log(1e-8)
+LIVE_LOG_MAX = F(0.0)
+
+
+def live_slices(u, positions, width, height, stride, slice_axis, color_axis, margin):
+    """_extract_live_vorticity_slices (tools/lbm3d_realtime_control.py:68-142): the vorticity
+    component `color_axis` on planes normal to `slice_axis` at `positions`, in-plane samples
+    p * stride (p < width) and q * stride (q < height) clamped to the grid, flattened as
+    (slice, q, p). A position outside the grid gives zeros (the CUDA kernel's rule; the
+    reference would index out of bounds). u: (3, nx, ny, nz) binary32."""
+    u = _f(u)
+    n = u.shape[1:]
+    out = np.zeros((len(positions), height, width), F)
+    P, Q = np.meshgrid(np.arange(width), np.arange(height))
+    for k, pos in enumerate(positions):
+        if not 0 <= pos < n[slice_axis]:
+            continue
+        full = np.full(P.shape, pos)
+        if slice_axis == 0:
+            x, y, z = full, np.minimum(P * stride, n[1] - 1), np.minimum(Q * stride, n[2] - 1)
+        elif slice_axis == 1:
+            x, y, z = np.minimum(P * stride, n[0] - 1), full, np.minimum(Q * stride, n[2] - 1)
+        else:
+            x, y, z = np.minimum(P * stride, n[0] - 1), np.minimum(Q * stride, n[1] - 1), full
+        xm, xp = np.maximum(x - 1, 0), np.minimum(x + 1, n[0] - 1)
+        ym, yp = np.maximum(y - 1, 0), np.minimum(y + 1, n[1] - 1)
+        zm, zp = np.maximum(z - 1, 0), np.minimum(z + 1, n[2] - 1)
+        inv_dx = F(1) / np.maximum(xp - xm, 1).astype(F)
+        inv_dy = F(1) / np.maximum(yp - ym, 1).astype(F)
+        inv_dz = F(1) / np.maximum(zp - zm, 1).astype(F)
+        if color_axis == 0:
+            v = (u[2][x, yp, z] - u[2][x, ym, z]) * inv_dy - (u[1][x, y, zp] - u[1][x, y, zm]) * inv_dz
+        elif color_axis == 1:
+            v = (u[0][x, y, zp] - u[0][x, y, zm]) * inv_dz - (u[2][xp, y, z] - u[2][xm, y, z]) * inv_dx
+        else:
+            v = (u[1][xp, y, z] - u[1][xm, y, z]) * inv_dx - (u[0][x, yp, z] - u[0][x, ym, z]) * inv_dy
+        edge = ((x < margin) | (x >= n[0] - margin) | (y < margin) | (y >= n[1] - margin) | (z < margin) |
+                (z >= n[2] - margin))
+        out[k] = np.where(edge, F(0), v)
+    return out.reshape(-1)
+
+
+def live_histogram(values):
+    """The 256-bin histogram of log|value| over [log 1e-8, log 1] for |value| > 1e-8
+    (tools/lbm3d_realtime_control.py:143-148), with the logarithm in binary64; and how many
+    values lie within 1e-4 of a bin edge (in bins), whose bin a binary32 logarithm may move."""
+    mag = np.abs(_f(values))
+    m = mag[mag > F(1e-8)].astype(np.float64)
+    c = np.clip((np.log(m) - float(LIVE_LOG_MIN)) / (float(LIVE_LOG_MAX) - float(LIVE_LOG_MIN)), 0.0, 0.999999)
+    pos = c * LIVE_BINS
+    hist = np.bincount(pos.astype(np.int64), minlength=LIVE_BINS)
+    frac = pos - np.floor(pos)
+    return hist, int(((frac < 1e-4) | (frac > 1 - 1e-4)).sum())
+
+
+def live_rgba(values, vmax, alpha):
+    """_live_vorticity_to_rgba (tools/lbm3d_realtime_control.py:157-182) in binary32: uint8
+    (n, 4)."""
+    v = _f(values)
+    t0 = np.clip(F(0.5) + F(0.5) * v / np.maximum(F(vmax), F(1e-8)), F(0), F(1))
+    low = t0 < F(0.5)
+    t_lo = t0 * F(2)
+    t_hi = (t0 - F(0.5)) * F(2)
+    r = np.where(low, F(255) * t_lo, F(255))
+    g = np.where(low, F(255) * t_lo, F(255) * (F(1) - t_hi))
+    b = np.where(low, F(255), F(255) * (F(1) - t_hi))
+    a = np.full_like(v, F(255) * np.clip(F(alpha), F(0), F(1)))
+    return np.stack([r, g, b, a], axis=1).astype(np.uint8)

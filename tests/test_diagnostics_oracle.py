@@ -51,3 +51,42 @@ def test_mesh_queries_on_a_triangle_and_a_closed_tetrahedron():
     tet = v[[[0, 2, 1], [0, 1, 3], [0, 3, 2], [1, 2, 3]]]
     assert od._crossings(tet, np.array([0.5, 0.5, 0.5], np.float32)) % 2 == 1
     assert od._crossings(tet, np.array([2.5, 2.5, 2.5], np.float32)) % 2 == 0
+
+
+def test_live_slices_oracle_on_linear_fields():
+    """The live view's vorticity of u = (a z, b x, c y) is (c, a, b) everywhere, border samples
+    (one-sided, divided by the clamped span) and clamped in-plane samples included; a position
+    outside the grid gives zeros; the margin zeroes the cells near a face."""
+    n = (6, 7, 8)
+    x, y, z = np.meshgrid(*(np.arange(k, dtype=np.float32) for k in n), indexing="ij")
+    u = np.stack([0.5 * z, 0.25 * x, 0.125 * y]).astype(np.float32)  # curl = (0.125, 0.5, 0.25)
+    for slice_axis in range(3):
+        for color_axis, want in enumerate((0.125, 0.5, 0.25)):
+            v = od.live_slices(u, [1, n[slice_axis] - 1, n[slice_axis]], 5, 6, 2, slice_axis, color_axis, 0)
+            v = v.reshape(3, 6, 5)
+            np.testing.assert_array_equal(v[:2], np.float32(want))
+            np.testing.assert_array_equal(v[2], 0)
+    m = od.live_slices(u, [3], 5, 6, 1, 2, 2, 1).reshape(6, 5)  # z = 3, x = p, y = q
+    np.testing.assert_array_equal(m[1:6, 1:5], np.float32(0.25))
+    assert (m[0] == 0).all() and (m[:, 0] == 0).all()
+
+
+def test_live_histogram_rgba_and_vmax():
+    from openhomelbm_b200 import diagnostics as dg
+
+    vals = np.array([0, 1e-9, 1e-8 * 1.01, 3e-4, -3e-4, 0.5, 2.0], np.float32)
+    h, amb = od.live_histogram(vals)
+    assert h.sum() == 5 and h[-1] == 1 and amb == 0  # 0.5 and 2 (clamped) share the top bins
+    assert h[int(np.clip((np.log(3e-4) + 18.420680743952367) / 18.420680743952367, 0, 0.999999) * 256)] == 2
+    assert od.live_histogram(np.array([1e-4], np.float32))[1] == 1  # log 1e-4 is a bin edge
+    rgba = od.live_rgba(np.array([-3, -0.5, 0, 0.5, 3], np.float32), 1.0, 0.5)
+    np.testing.assert_array_equal(rgba[:, 3], 127)
+    np.testing.assert_array_equal(rgba[[0, 2, 4], :3], [[0, 0, 255], [255, 255, 255], [255, 0, 0]])
+    counts = np.zeros(256, np.int64)
+    counts[100] = 10
+    want = np.exp(-18.420680743952367 * (1 - 100.5 / 256))
+    assert abs(dg.vmax_from_histogram(counts, 98.0) - want) < 1e-12 * want
+    assert dg.vmax_from_histogram(np.zeros(256), 98.0) == 1e-6
+    assert dg.vmax_from_histogram(counts, 98.0, previous=10 * want) == 9.6 * want
+    counts[200] = 1  # the 98th percentile of 11 counts is the 11th: bin 200
+    assert abs(dg.vmax_from_histogram(counts, 98.0) - np.exp(-18.420680743952367 * (1 - 200.5 / 256))) < 1e-9

@@ -122,3 +122,37 @@ def test_image_entry_points_reject_bad_arguments():
     s3, f3 = _world3d()
     with pytest.raises(ValueError):
         dg.get_u_img_xy_3d(f3, f3.nz)  # slice outside the grid
+
+
+@pytest.mark.parametrize("slice_axis,color_axis,margin", [(2, 2, 0), (0, 1, 2), (1, 0, 1)])
+def test_live_slices_histogram_and_rgba_match_oracle(slice_axis, color_axis, margin):
+    from openhomelbm_b200 import diagnostics as dg
+
+    s, f = _world3d()
+    u = f.decoded()[1:4].float().cpu().numpy()
+    n = (f.nx, f.ny, f.nz)
+    inplane = [a for a in range(3) if a != slice_axis]
+    stride = 2
+    W, H = n[inplane[0]] // stride + 2, n[inplane[1]] // stride + 2  # samples past the edge clamp
+    # the flow (started at rest, inflow at x = 0) has reached the first few x planes only;
+    # the last position lies outside the grid
+    positions = [3, n[slice_axis] // 2, n[slice_axis] - 1, n[slice_axis] + 3]
+    pos = torch.tensor(positions, dtype=torch.int32, device=f.device)
+    values = torch.full((len(positions) * W * H,), 7.0, device=f.device)
+    hist = torch.ones(256, dtype=torch.int32, device=f.device)
+    dg.clear_live_histogram(hist)
+    dg.extract_live_vorticity_slices(f, pos, values, hist, W, H, stride, slice_axis, color_axis, margin, 1)
+    ref = od.live_slices(u, positions, W, H, stride, slice_axis, color_axis, margin)
+    np.testing.assert_array_equal(values.cpu().numpy(), ref)
+    h_ref, ambiguous = od.live_histogram(ref)
+    h = hist.cpu().numpy()
+    assert h_ref.sum() > 20 and h.sum() == h_ref.sum()
+    assert np.abs(h - h_ref).sum() <= 2 * ambiguous
+    vmax = dg.vmax_from_histogram(h, 98.0)
+    rgba = torch.zeros(values.numel() * 4, dtype=torch.uint8, device=f.device)
+    dg.live_vorticity_to_rgba(values, rgba, vmax, 0.8)
+    np.testing.assert_array_equal(rgba.cpu().numpy().reshape(-1, 4), od.live_rgba(ref, vmax, 0.8))
+    # without collecting, the histogram is left alone
+    before = hist.clone()
+    dg.extract_live_vorticity_slices(f, pos, values, hist, W, H, stride, slice_axis, color_axis, margin, 0)
+    assert torch.equal(hist, before)
