@@ -435,6 +435,18 @@ HL_API int hl_d3q27_live_slices(const hl_world3d* w, const int32_t* slice_positi
                                 int collect_histogram, float* values, int32_t* histogram, hl_stream stream);
 HL_API int hl_live_rgba(const float* values, long long n, float vmax, float alpha, uint8_t* rgba, hl_stream stream);
 
+/* The 2D realtime tool's GPU kernels (tools/lbm2d_realtime_control.py), headless:
+ *  - hl_d2q9_uimg_rgba (lbm_uimg_to_rgba_kernel 417-464): an (nx, ny) image, e.g. u_img, to
+ *    RGBA bytes laid out (ny, nx, 4); render_mode 0 velocity magnitude over vmax, 1 vorticity
+ *    over +-vmax (values >= 999 grey), 2 solid boundary.
+ *  - hl_d2q9_local_force (set_local_force_kernel 144-157): forcex/forcey (nx, ny) =
+ *    (fx, fy) * max(0, 1 - ((x - cx)/rx)^2 - ((y - cy)/ry)^2).
+ * Stream-ordered, allocation-free, capturable. */
+HL_API int hl_d2q9_uimg_rgba(const float* u_img, int nx, int ny, int render_mode, float vmax, uint8_t* rgba,
+                             hl_stream stream);
+HL_API int hl_d2q9_local_force(float* forcex, float* forcey, int nx, int ny, float cx, float cy, float rx, float ry,
+                               float fx, float fy, hl_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -86,6 +86,9 @@ _SIGS = {
     "hl_d3q27_live_slices": ([POINTER(hl_world3d), c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int,
                               c_void_p, c_void_p, c_void_p], c_int),
     "hl_live_rgba": ([c_void_p, c_longlong, c_float, c_float, c_void_p, c_void_p], c_int),
+    "hl_d2q9_uimg_rgba": ([c_void_p, c_int, c_int, c_int, c_float, c_void_p, c_void_p], c_int),
+    "hl_d2q9_local_force": ([c_void_p, c_void_p, c_int, c_int, c_float, c_float, c_float, c_float, c_float, c_float,
+                             c_void_p], c_int),
     "hl_d3q27_batch_bytes": ([c_int], c_size_t),
     "hl_d3q27_batch_prepare": ([POINTER(hl_world3d), c_int, c_void_p, c_size_t, POINTER(c_int), c_void_p], c_int),
     "hl_d3q27_stream_collide_batch": ([c_void_p, c_int, c_int, c_double, POINTER(hl_storage), c_int, c_void_p,

@@ -9,7 +9,8 @@
 //      any_mesh_hit_along_ray_3d 320-362.
 //   live view (tools/lbm3d_realtime_control.py): _extract_live_vorticity_slices 68-148 with
 //      its log-magnitude histogram, _live_vorticity_to_rgba 157-182 (into a device RGBA buffer
-//      instead of the GL atlas).
+//      instead of the GL atlas); tools/lbm2d_realtime_control.py: lbm_uimg_to_rgba_kernel
+//      417-464 (into a device buffer instead of the GL PBO), set_local_force_kernel 144-157.
 // Velocities are the decoded u of the current buffer, in binary32 as the reference's fields.
 //
 // Third-party queries of the reference, restated: wp.mesh_query_ray (any hit with
@@ -485,6 +486,56 @@ __global__ void __launch_bounds__(BLOCK) live_rgba_kernel(const float* values, u
   px[3] = uint8_t(255.f * fminf(fmaxf(alpha, 0.f), 1.f));
 }
 
+// ------------------------------------------------------------------- 2D realtime view
+__device__ __forceinline__ float clamp01(float v) { return fminf(fmaxf(v, 0.f), 1.f); }
+
+// u_img (nx, ny) to RGBA bytes laid out (ny, nx, 4): render_mode 0 |u| on a dark-red-yellow
+// ramp, 1 vorticity blue-white-red (values >= 999, the solid mark, light grey), 2 solid
+// boundary as ink on white; alpha 255.
+__global__ void __launch_bounds__(BLOCK) uimg_rgba_kernel(const float* img, int nx, int ny, int mode, float vmax,
+                                                          uint8_t* out) {
+  const long long i = (long long)blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= (long long)nx * ny) return;
+  const int x = int(i / ny), y = int(i - (long long)x * ny);
+  const float val = img[i];
+  float r, g, b;
+  if (mode == 2) {
+    const float c = (1.f - clamp01(val)) * 255.f;
+    r = c, g = c, b = c;
+  } else if (mode == 1) {
+    if (val >= 999.f) {
+      r = 200.f, g = 200.f, b = 200.f;
+    } else {
+      const float n = clamp01(0.5f + 0.5f * val / fmaxf(vmax, 1.0e-6f));
+      if (n < 0.5f) {
+        const float t = n * 2.f;
+        r = 255.f * t, g = 255.f * t, b = 255.f;
+      } else {
+        const float t = (n - 0.5f) * 2.f;
+        r = 255.f, g = 255.f * (1.f - t), b = 255.f * (1.f - t);
+      }
+    }
+  } else {
+    const float n = clamp01(val / fmaxf(vmax, 1.0e-6f));
+    r = 255.f * n, g = 180.f * n * n, b = 60.f * (1.f - n);
+  }
+  uint8_t* px = out + ((long long)y * nx + x) * 4;
+  px[0] = uint8_t(r), px[1] = uint8_t(g), px[2] = uint8_t(b), px[3] = 255;
+}
+
+// A force field that falls off over an ellipse: f (1 - r^2) inside, 0 outside.
+__global__ void __launch_bounds__(BLOCK) local_force_kernel(float* fxo, float* fyo, int nx, int ny, float cx, float cy,
+                                                            float rx, float ry, float fx, float fy) {
+  const long long i = (long long)blockIdx.x * BLOCK + threadIdx.x;
+  if (i >= (long long)nx * ny) return;
+  const int x = int(i / ny), y = int(i - (long long)x * ny);
+  const float dx = (float(x) - cx) / fmaxf(rx, 1.0e-6f);
+  const float dy = (float(y) - cy) / fmaxf(ry, 1.0e-6f);
+  const float w = fmaxf(0.f, 1.f - (dx * dx + dy * dy));
+  fxo[i] = fx * w;
+  fyo[i] = fy * w;
+}
+
 template <class S, class A, class K> int launch(K kern, const A& a, long long pixels, cudaStream_t st) {
   if (pixels == 0) return HL_OK;
   kern<<<unsigned((pixels + BLOCK - 1) / BLOCK), BLOCK, 0, st>>>(a);
@@ -612,5 +663,28 @@ extern "C" int hl_live_rgba(const float* values, long long n, float vmax, float 
   diag::live_rgba_kernel<<<unsigned((n + diag::BLOCK - 1) / diag::BLOCK), diag::BLOCK, 0, st>>>(values, rgba, n, vmax,
                                                                                                  alpha);
   HL_LAUNCH_CHECK("live rgba");
+  return HL_OK;
+}
+
+extern "C" int hl_d2q9_uimg_rgba(const float* u_img, int nx, int ny, int render_mode, float vmax, uint8_t* rgba,
+                                 hl_stream stream) {
+  HL_CHECK_ARG(u_img != nullptr && rgba != nullptr, "uimg rgba: image or rgba is NULL");
+  HL_CHECK_ARG(nx >= 1 && ny >= 1, "uimg rgba: image %d x %d", nx, ny);
+  HL_CHECK_ARG(render_mode >= 0 && render_mode <= 2, "uimg rgba: render mode %d (0, 1, 2)", render_mode);
+  const long long n = (long long)nx * ny;
+  diag::uimg_rgba_kernel<<<unsigned((n + diag::BLOCK - 1) / diag::BLOCK), diag::BLOCK, 0,
+                           static_cast<cudaStream_t>(stream)>>>(u_img, nx, ny, render_mode, vmax, rgba);
+  HL_LAUNCH_CHECK("uimg rgba");
+  return HL_OK;
+}
+
+extern "C" int hl_d2q9_local_force(float* forcex, float* forcey, int nx, int ny, float cx, float cy, float rx,
+                                   float ry, float fx, float fy, hl_stream stream) {
+  HL_CHECK_ARG(forcex != nullptr && forcey != nullptr, "local force: force field is NULL");
+  HL_CHECK_ARG(nx >= 1 && ny >= 1, "local force: grid %d x %d", nx, ny);
+  const long long n = (long long)nx * ny;
+  diag::local_force_kernel<<<unsigned((n + diag::BLOCK - 1) / diag::BLOCK), diag::BLOCK, 0,
+                             static_cast<cudaStream_t>(stream)>>>(forcex, forcey, nx, ny, cx, cy, rx, ry, fx, fy);
+  HL_LAUNCH_CHECK("local force");
   return HL_OK;
 }

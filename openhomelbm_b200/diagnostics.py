@@ -219,3 +219,18 @@ def vmax_from_histogram(counts, percentile: float, previous=None) -> float:
         fraction = (min(bin_id, _LIVE_HISTOGRAM_BINS - 1) + 0.5) / _LIVE_HISTOGRAM_BINS
         current = math.exp(_LIVE_LOG_VORT_MIN + fraction * (_LIVE_LOG_VORT_MAX - _LIVE_LOG_VORT_MIN))
     return max(current, 1.0e-8) if previous is None else max(previous * 0.96, current, 1.0e-8)
+
+
+def lbm_uimg_to_rgba(flow, out: torch.Tensor, render_mode: int, vmax: float) -> torch.Tensor:
+    """lbm_uimg_to_rgba_kernel (tools/lbm2d_realtime_control.py:417-464): flow.u_img (nx, ny)
+    to RGBA bytes in `out` (uint8, (ny, nx, 4)); render_mode 0 velocity, 1 vorticity (solid
+    marks grey), 2 solid boundary. A device buffer stands in for the GL pixel buffer."""
+    img = getattr(flow, "u_img", None)
+    if img is None or tuple(img.shape) != (flow.nx, flow.ny):
+        raise ValueError("lbm_uimg_to_rgba: flow.u_img is not filled (call get_u_img or another 2D image first)")
+    if out.dtype != torch.uint8 or tuple(out.shape) != (flow.ny, flow.nx, 4) or not out.is_contiguous() \
+            or out.device != img.device:
+        raise ValueError("lbm_uimg_to_rgba: out must be a contiguous uint8 (ny, nx, 4) tensor on the world's device")
+    _lib.check(_lib.lib().hl_d2q9_uimg_rgba(img.data_ptr(), flow.nx, flow.ny, int(render_mode), float(vmax),
+                                            out.data_ptr(), _lib.stream_ptr()), "uimg rgba")
+    return out

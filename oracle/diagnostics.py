@@ -363,3 +363,38 @@ def live_rgba(values, vmax, alpha):
     b = np.where(low, F(255), F(255) * (F(1) - t_hi))
     a = np.full_like(v, F(255) * np.clip(F(alpha), F(0), F(1)))
     return np.stack([r, g, b, a], axis=1).astype(np.uint8)
+
+
+# ---------------------------------------------------------------------- 2D realtime view
+def uimg_rgba(img, mode, vmax):
+    """lbm_uimg_to_rgba_kernel (tools/lbm2d_realtime_control.py:417-464) in binary32: uint8
+    (ny, nx, 4) from an (nx, ny) image."""
+    v = _f(img)
+    if mode == 2:
+        c = (F(1) - np.clip(v, F(0), F(1))) * F(255)
+        r = g = b = c
+    elif mode == 1:
+        n = np.clip(F(0.5) + F(0.5) * v / np.maximum(F(vmax), F(1e-6)), F(0), F(1))
+        lo = n < F(0.5)
+        t_lo, t_hi = n * F(2), (n - F(0.5)) * F(2)
+        r = np.where(lo, F(255) * t_lo, F(255))
+        g = np.where(lo, F(255) * t_lo, F(255) * (F(1) - t_hi))
+        b = np.where(lo, F(255), F(255) * (F(1) - t_hi))
+        solid = v >= F(999)
+        r, g, b = (np.where(solid, F(200), c) for c in (r, g, b))
+    else:
+        n = np.clip(v / np.maximum(F(vmax), F(1e-6)), F(0), F(1))
+        r, g, b = F(255) * n, F(180) * n * n, F(60) * (F(1) - n)
+    out = np.stack([r, g, b, np.full_like(v, F(255))], axis=-1).astype(np.uint8)
+    return np.ascontiguousarray(out.transpose(1, 0, 2))
+
+
+def local_force(nx, ny, cx, cy, rx, ry, fx, fy):
+    """set_local_force_kernel (tools/lbm2d_realtime_control.py:144-157) in binary32:
+    (forcex, forcey), each (nx, ny)."""
+    x = np.arange(nx, dtype=F)[:, None]
+    y = np.arange(ny, dtype=F)[None, :]
+    dx = (x - F(cx)) / np.maximum(F(rx), F(1e-6))
+    dy = (y - F(cy)) / np.maximum(F(ry), F(1e-6))
+    w = np.maximum(F(0), F(1) - (dx * dx + dy * dy))
+    return F(fx) * w, F(fy) * w

@@ -90,3 +90,19 @@ def test_live_histogram_rgba_and_vmax():
     assert dg.vmax_from_histogram(counts, 98.0, previous=10 * want) == 9.6 * want
     counts[200] = 1  # the 98th percentile of 11 counts is the 11th: bin 200
     assert abs(dg.vmax_from_histogram(counts, 98.0) - np.exp(-18.420680743952367 * (1 - 200.5 / 256))) < 1e-9
+
+
+def test_2d_realtime_oracle_maps():
+    img = np.array([[0.0, 0.5], [1.0, 2.0]], np.float32)  # (nx, ny)
+    out = od.uimg_rgba(img, 0, 1.0)
+    assert out.shape == (2, 2, 4) and (out[..., 3] == 255).all()
+    np.testing.assert_array_equal(out[0, 0, :3], [0, 0, 60])      # x 0, y 0: zero
+    np.testing.assert_array_equal(out[1, 0, :3], [127, 45, 30])   # x 0, y 1: half
+    np.testing.assert_array_equal(out[0, 1, :3], [255, 180, 0])   # x 1, y 0: full
+    v = od.uimg_rgba(np.array([[-1.0, 1000.0], [0.0, 1.0]], np.float32), 1, 1.0)
+    # (y, x) order: (0, 0) -1 blue, (0, 1) 0 white, (1, 0) the solid mark grey, (1, 1) 1 red
+    np.testing.assert_array_equal(v[:, :, :3].reshape(-1, 3), [[0, 0, 255], [255, 255, 255], [200, 200, 200],
+                                                               [255, 0, 0]])
+    np.testing.assert_array_equal(od.uimg_rgba(np.array([[0.0, 0.25]], np.float32), 2, 1.0)[:, 0, 0], [255, 191])
+    fx, fy = od.local_force(5, 5, 2, 2, 2, 2, 1.0, -2.0)
+    assert fx[2, 2] == 1.0 and fy[2, 2] == -2.0 and fx[0, 0] == 0 and fx[2, 3] == np.float32(0.75)

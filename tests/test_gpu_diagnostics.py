@@ -156,3 +156,40 @@ def test_live_slices_histogram_and_rgba_match_oracle(slice_axis, color_axis, mar
     before = hist.clone()
     dg.extract_live_vorticity_slices(f, pos, values, hist, W, H, stride, slice_axis, color_axis, margin, 0)
     assert torch.equal(hist, before)
+
+
+def test_2d_realtime_rgba_and_controls():
+    """The 2D realtime tool's GPU kernels: u_img to RGBA in the three render modes, the local
+    force field, and the boundary-velocity and prescribed-motion controls."""
+    from openhomelbm_b200 import diagnostics as dg
+    from openhomelbm_b200.lbm import controls
+
+    s, f = _world2d("float32")
+    fills = ((0, dg.get_u_img), (1, lambda fl: dg.get_vorticity_with_solid_img(fl, 1.5)),
+             (2, lambda fl: dg.get_solid_boundary_img(fl, 1.5)))
+    for mode, fill in fills:
+        img = fill(f).cpu().numpy()
+        vmax = {0: 0.06, 1: float(np.abs(img[img < 999]).max()) * 0.5, 2: 1.0}[mode]
+        out = torch.zeros((f.ny, f.nx, 4), dtype=torch.uint8, device=f.device)
+        dg.lbm_uimg_to_rgba(f, out, mode, vmax)
+        np.testing.assert_array_equal(out.cpu().numpy(), od.uimg_rgba(img, mode, vmax))
+        if mode == 1:
+            assert (out.cpu().numpy()[..., 0] == 200).sum() > 20  # the solid marks
+    controls.set_local_force(s.flows, 30.5, 20.0, 6.0, 4.0, 1e-5, -2e-5)
+    fx, fy = od.local_force(f.nx, f.ny, 30.5, 20.0, 6.0, 4.0, 1e-5, -2e-5)
+    np.testing.assert_array_equal(f.force[0].cpu().numpy(), fx)
+    np.testing.assert_array_equal(f.force[1].cpu().numpy(), fy)
+    assert f.use_force and (fx > 0).sum() > 50
+    controls.set_boundary_velocity(s.flows, 0, 0.03, 0.01)
+    np.testing.assert_allclose(f.bc_value[0], [0.03, 0.01], rtol=1e-6)
+    p0, a0 = f.solid_position[1].clone(), float(f.solid_angle[1])
+    controls.advance_prescribed_solid_motion(s.flows, 1, 0.5, -0.25, 0.1)
+    torch.testing.assert_close(f.solid_position[1], p0 + torch.tensor([0.5, -0.25], device=f.device))
+    assert abs(float(f.solid_angle[1]) - (a0 + 0.1)) < 1e-6
+    s.step()  # forced, new inflow, moved solid
+    torch.cuda.synchronize()
+    assert torch.isfinite(f.decoded()).all()
+    with pytest.raises(ValueError):
+        controls.set_boundary_velocity(s.flows, 4, 0.0, 0.0)
+    with pytest.raises(ValueError):
+        dg.lbm_uimg_to_rgba(f, torch.zeros((f.nx, f.ny, 4), dtype=torch.uint8, device=f.device), 0, 0.1)
