@@ -235,6 +235,24 @@ HL_API int hl_d3q27_solid_links(const hl_world3d* w, double vis_shear, const hl_
  * at most max_bound_radius. */
 HL_API size_t hl_d3q27_solid_links_work_ints(int n_objects, float max_bound_radius);
 
+/* The cut links of many domains in one classify and one process launch (the serving form;
+ * the reference runs each world's step on its own). Per cell the same computation as
+ * hl_d3q27_solid_links; each domain's loads are its binary64 sums and binary32 force/torque.
+ *  - hl_d3q27_links_batch_bytes(n, total solids): device bytes of the descriptors.
+ *  - hl_d3q27_links_batch_prepare: writes the descriptors of worlds[k] / solids[k] (parity 0
+ *    reads cur, parity 1 reads post; the solids' force / torque pointers are where this
+ *    descriptor set writes the loads) into desc (64-byte aligned device memory) and sets
+ *    *work_ints, the int32 work list the launches need. One storage type for all domains.
+ *    Synchronises the stream; prepare again when any pointer changes.
+ *  - hl_d3q27_solid_links_batch: one pass at `parity`, after the domains' stream-collide
+ *    (batched or not). Capturable. */
+HL_API size_t hl_d3q27_links_batch_bytes(int n_domains, int n_solids_total);
+HL_API int hl_d3q27_links_batch_prepare(const hl_world3d* worlds, const hl_solids3d* solids, int n_domains,
+                                        double vis_shear, void* desc, size_t desc_bytes, size_t* work_ints,
+                                        hl_stream stream);
+HL_API int hl_d3q27_solid_links_batch(const void* desc, int n_domains, int parity, int32_t* work, size_t work_ints,
+                                      hl_stream stream);
+
 /* ------------------------------------------------------------------ coupling
  * The MuJoCo-Warp coupling kernels of the environments, over batched per-world arrays:
  * a per-solid array of nworld worlds is [nworld][n_objects][...] with world stride

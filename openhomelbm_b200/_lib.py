@@ -89,6 +89,10 @@ _SIGS = {
     "hl_d2q9_uimg_rgba": ([c_void_p, c_int, c_int, c_int, c_float, c_void_p, c_void_p], c_int),
     "hl_d2q9_local_force": ([c_void_p, c_void_p, c_int, c_int, c_float, c_float, c_float, c_float, c_float, c_float,
                              c_void_p], c_int),
+    "hl_d3q27_links_batch_bytes": ([c_int, c_int], c_size_t),
+    "hl_d3q27_links_batch_prepare": ([POINTER(hl_world3d), POINTER(hl_solids3d), c_int, c_double, c_void_p, c_size_t,
+                                      POINTER(c_size_t), c_void_p], c_int),
+    "hl_d3q27_solid_links_batch": ([c_void_p, c_int, c_int, c_void_p, c_size_t, c_void_p], c_int),
     "hl_d3q27_batch_bytes": ([c_int], c_size_t),
     "hl_d3q27_batch_prepare": ([POINTER(hl_world3d), c_int, c_void_p, c_size_t, POINTER(c_int), c_void_p], c_int),
     "hl_d3q27_stream_collide_batch": ([c_void_p, c_int, c_int, c_double, POINTER(hl_storage), c_int, c_void_p,

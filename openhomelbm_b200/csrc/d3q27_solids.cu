@@ -42,6 +42,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
 
 #include "hl_common.cuh"
 #include "mesh_geom.cuh"
@@ -535,31 +539,35 @@ template <class S> __global__ void __launch_bounds__(BLOCK) band_kernel(const __
 // one at a time from a shared counter, a cell per warp as in band_kernel, so that a warp held
 // by an expensive cell (near a joint, hundreds of candidate triangles) takes no others.
 constexpr int WORK_HEAD = 4;
-template <class S> __global__ void __launch_bounds__(BLOCK) classify_kernel(const __grid_constant__ Args a) {
-  using R = typename S::R;
+// Cell idx of solid k0's band box: its index c in the world and the mask of the solids whose
+// triangles a link of it could reach (0: not a candidate cut cell, or not this solid's to do).
+__device__ __forceinline__ unsigned classify_cell(const Args& a, int k0, long long idx, int& c) {
   const hl_solids3d& s = a.s;
-  const int k0 = blockIdx.y;
   const int nx = a.w.nx, ny = a.w.ny, nz = a.w.nz;
   const float px = s.position[3 * k0], py = s.position[3 * k0 + 1], pz = s.position[3 * k0 + 2];
   const float r = s.bound_radius[k0] + 2.f;
   const int side = a.box_side;
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  bool flagged = false;
-  int c = 0;
-  unsigned solids = 0u;
-  if (s.tri_offset[k0 + 1] > s.tri_offset[k0] && isfinite(px) && isfinite(py) && isfinite(pz) && isfinite(r) &&
-      idx < (long long)side * side * side) {
-    const int x = int(floorf(px - r)) + int(idx / ((long long)side * side));
-    const int y = int(floorf(py - r)) + int((idx / side) % side);
-    const int z = int(floorf(pz - r)) + int(idx % side);
-    const bool inside = x >= 0 && x < nx && y >= 0 && y < ny && z >= 0 && z < nz;
-    c = (x * ny + y) * nz + z;
-    const bool fluid = inside && (a.w.flag == nullptr || a.w.flag[c] == ML_FLUID) &&
-                       (a.w.flag != nullptr || a.w.periodic || (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1));
-    if (fluid && first_near<float>(s, float(x), float(y), float(z)) == k0)
-      solids = cut_mask<float>(s, V3<float>{float(x), float(y), float(z)});
-    flagged = solids != 0u;
-  }
+  c = 0;
+  if (!(s.tri_offset[k0 + 1] > s.tri_offset[k0] && isfinite(px) && isfinite(py) && isfinite(pz) && isfinite(r) &&
+        idx < (long long)side * side * side))
+    return 0u;
+  const int x = int(floorf(px - r)) + int(idx / ((long long)side * side));
+  const int y = int(floorf(py - r)) + int((idx / side) % side);
+  const int z = int(floorf(pz - r)) + int(idx % side);
+  const bool inside = x >= 0 && x < nx && y >= 0 && y < ny && z >= 0 && z < nz;
+  c = (x * ny + y) * nz + z;
+  const bool fluid = inside && (a.w.flag == nullptr || a.w.flag[c] == ML_FLUID) &&
+                     (a.w.flag != nullptr || a.w.periodic || (x > 0 && x < nx - 1 && y > 0 && y < ny - 1 && z > 0 && z < nz - 1));
+  if (fluid && first_near<float>(s, float(x), float(y), float(z)) == k0)
+    return cut_mask<float>(s, V3<float>{float(x), float(y), float(z)});
+  return 0u;
+}
+
+template <class S> __global__ void __launch_bounds__(BLOCK) classify_kernel(const __grid_constant__ Args a) {
+  const hl_solids3d& s = a.s;
+  int c;
+  const unsigned solids = classify_cell(a, blockIdx.y, (long long)blockIdx.x * blockDim.x + threadIdx.x, c);
+  const bool flagged = solids != 0u;
   const unsigned mask = __ballot_sync(0xffffffffu, flagged);
   if (mask == 0) return;
   const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
@@ -622,6 +630,85 @@ __global__ void loads_out_kernel(hl_solids3d s) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < s.n_objects) loads_out(s, k);
 }
+
+// ------------------------------------------------------------------ batched domains
+// The cut links of many domains in one classify and one process launch. Descriptor layout
+// in device memory: a BatchHead, the per-domain Args for parity 0 then for parity 1 (parity p
+// reads buffer p), then the classify launch's block rows, one (domain, solid) pair each. The
+// work list holds LB_HEAD counters (entries, finished process blocks, next entry, unused) and
+// (domain, cell, solid mask) entries.
+constexpr int LB_HEAD = 4;
+struct BatchHead {
+  int n_domains, n_rows, max_box, pad;
+};
+__host__ __device__ constexpr size_t align64(size_t b) { return (b + 63) / 64 * 64; }
+constexpr size_t LB_ARGS_OFF = align64(sizeof(BatchHead));
+__host__ __device__ inline size_t lb_rows_off(int n) { return LB_ARGS_OFF + align64(2 * size_t(n) * sizeof(Args)); }
+
+template <class S>
+__global__ void __launch_bounds__(BLOCK) classify_batch_kernel(const unsigned char* __restrict__ desc, int parity,
+                                                               int32_t* work) {
+  const BatchHead& h = *reinterpret_cast<const BatchHead*>(desc);
+  const Args* args = reinterpret_cast<const Args*>(desc + LB_ARGS_OFF) + size_t(parity) * h.n_domains;
+  const int2 row = reinterpret_cast<const int2*>(desc + lb_rows_off(h.n_domains))[blockIdx.y];
+  const Args& a = args[row.x];
+  if (blockIdx.x == 0 && threadIdx.x < 6) a.s.loads64[6 * row.y + threadIdx.x] = 0.0;  // once per solid
+  int c;
+  const unsigned solids = classify_cell(a, row.y, (long long)blockIdx.x * blockDim.x + threadIdx.x, c);
+  const bool flagged = solids != 0u;
+  const unsigned mask = __ballot_sync(FULL, flagged);
+  if (mask == 0) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(work, __popc(mask));
+  base = __shfl_sync(FULL, base, leader);
+  if (flagged) {
+    int32_t* e = work + LB_HEAD + 3 * (base + __popc(mask & ((1u << lane) - 1)));
+    e[0] = row.x, e[1] = c, e[2] = int(solids);
+  }
+}
+
+// Warps take the listed cells in turn; a cell's loads go straight to its domain's binary64
+// sums (zeroed by the classify launch); the last block writes every domain's binary32 loads.
+template <class S>
+__global__ void __launch_bounds__(BLOCK) process_batch_kernel(const unsigned char* __restrict__ desc, int parity,
+                                                              int32_t* work) {
+  __shared__ WarpScratch scratch[BLOCK / 32];
+  __shared__ bool last;
+  const BatchHead& h = *reinterpret_cast<const BatchHead*>(desc);
+  const Args* args = reinterpret_cast<const Args*>(desc + LB_ARGS_OFF) + size_t(parity) * h.n_domains;
+  const int count = work[0];
+  for (;;) {
+    int j = 0;
+    if ((threadIdx.x & 31) == 0) j = atomicAdd(work + 2, 1);
+    j = __shfl_sync(FULL, j, 0);
+    if (j >= count) break;
+    const int32_t* e = work + LB_HEAD + 3 * j;
+    const Args& a = args[e[0]];
+    const int c = e[1], ny = a.w.ny, nz = a.w.nz;
+    cut_cell<S>(a, a.s.loads64, scratch[threadIdx.x >> 5], c / (ny * nz), (c / nz) % ny, c % nz, unsigned(e[2]));
+    __syncwarp();
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(reinterpret_cast<unsigned*>(work + 1), 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int d = 0; d < h.n_domains; ++d)
+    for (int k = threadIdx.x; k < args[d].s.n_objects; k += blockDim.x) loads_out(args[d].s, k);
+}
+
+// prepared descriptors: address -> (domains, rows, largest band box side, work ints, dtype)
+struct BatchInfo {
+  int n_domains, n_rows, max_box;
+  size_t work_ints;
+  hl_dtype dtype;
+};
+std::mutex g_lb_mu;
+std::map<const void*, BatchInfo> g_lb;
+
+template <class S> int launch_batch(const void* desc, const BatchInfo& b, int parity, int32_t* work, cudaStream_t st);
 
 int num_sms_local() {
   static int n = 0;
@@ -701,4 +788,112 @@ extern "C" size_t hl_d3q27_solid_links_work_ints(int n_objects, float max_bound_
   const size_t side = size_t(d3s::box_side_of(max_bound_radius));
   // header (listed cells, finished blocks, next cell, unused), then (cell, solid mask) pairs
   return d3s::WORK_HEAD + 2 * size_t(n_objects) * side * side * side;
+}
+
+namespace hl {
+namespace d3s {
+template <class S> int launch_batch(const void* desc, const BatchInfo& b, int parity, int32_t* work, cudaStream_t st) {
+  const auto* d = static_cast<const unsigned char*>(desc);
+  const long long cells = (long long)b.max_box * b.max_box * b.max_box;
+  classify_batch_kernel<S><<<dim3(unsigned((cells + BLOCK - 1) / BLOCK), unsigned(b.n_rows)), BLOCK, 0, st>>>(d, parity,
+                                                                                                          work);
+  HL_LAUNCH_CHECK("d3q27 solid links batch (classify)");
+  const int blocks = g_tune_d3_link_blocks > 0 ? g_tune_d3_link_blocks : 4 * num_sms_local();
+  process_batch_kernel<S><<<unsigned(blocks), BLOCK, 0, st>>>(d, parity, work);
+  HL_LAUNCH_CHECK("d3q27 solid links batch (cut cells)");
+  return HL_OK;
+}
+}  // namespace d3s
+}  // namespace hl
+
+extern "C" size_t hl_d3q27_links_batch_bytes(int n_domains, int n_solids_total) {
+  if (n_domains <= 0 || n_solids_total < 0) return 0;
+  return d3s::lb_rows_off(n_domains) + size_t(n_solids_total) * sizeof(int2);
+}
+
+extern "C" int hl_d3q27_links_batch_prepare(const hl_world3d* worlds, const hl_solids3d* solids, int n_domains,
+                                            double vis_shear, void* desc, size_t desc_bytes, size_t* work_ints,
+                                            hl_stream stream) {
+  HL_CHECK_ARG(worlds != nullptr && solids != nullptr && work_ints != nullptr, "links batch: NULL argument");
+  HL_CHECK_ARG(n_domains >= 1 && n_domains <= 4096, "links batch: %d domains (1 .. 4096)", n_domains);
+  HL_CHECK_ARG(vis_shear > 0.0, "links batch: viscosity must be positive");
+  HL_CHECK_ARG(desc != nullptr && (reinterpret_cast<uintptr_t>(desc) & 63) == 0,
+               "links batch: descriptor buffer NULL or not 64-byte aligned");
+  std::vector<d3s::Args> args(2 * size_t(n_domains));
+  std::vector<int2> rows;
+  size_t capacity = 0;
+  int max_box = 0;
+  for (int k = 0; k < n_domains; ++k) {
+    const hl_world3d& w = worlds[k];
+    const hl_solids3d& s = solids[k];
+    HL_CHECK_ARG(w.nx >= 1 && w.ny >= 1 && w.nz >= 1 && w.cur && w.post && w.cur != w.post,
+                 "links batch: domain %d world", k);
+    HL_CHECK_ARG(w.storage.dtype == worlds[0].storage.dtype, "links batch: domain %d has another storage type", k);
+    HL_CHECK_ARG(s.n_objects >= 1 && s.n_objects <= d3s::MAX_SOLIDS, "links batch: domain %d has %d solids", k,
+                 s.n_objects);
+    HL_CHECK_ARG(s.tri_offset && s.tris && s.transforms && s.transforms_last && s.initialized && s.scale_sizes &&
+                     s.position && s.bound_radius && s.linear_v && s.angle_v && s.loads64,
+                 "links batch: domain %d: a solid field is NULL", k);
+    HL_CHECK_ARG(std::isfinite(s.max_bound_radius) && s.max_bound_radius >= 0.f && s.max_bound_radius < 512.f,
+                 "links batch: domain %d: max_bound_radius out of range", k);
+    for (int p = 0; p < 2; ++p) {
+      d3s::Args& a = args[size_t(p) * n_domains + k];
+      a.w = w;
+      if (p == 1) {
+        a.w.cur = w.post;
+        a.w.post = const_cast<void*>(w.cur);
+      }
+      a.vis_shear = vis_shear;
+      a.s = s;
+      a.s.work = nullptr;
+      a.sc = make_scale(w.storage);
+      a.box_side = d3s::box_side_of(s.max_bound_radius);
+    }
+    const int box = d3s::box_side_of(s.max_bound_radius);
+    max_box = std::max(max_box, box);
+    capacity += size_t(s.n_objects) * box * box * box;
+    for (int j = 0; j < s.n_objects; ++j) rows.push_back(make_int2(k, j));
+  }
+  HL_CHECK_ARG(rows.size() <= 65535, "links batch: %zu solids in all (at most 65535)", rows.size());
+  HL_CHECK_ARG(desc_bytes >= hl_d3q27_links_batch_bytes(n_domains, int(rows.size())),
+               "links batch: descriptor buffer too small");
+  std::vector<unsigned char> h(hl_d3q27_links_batch_bytes(n_domains, int(rows.size())), 0);
+  d3s::BatchHead head{n_domains, int(rows.size()), max_box, 0};
+  std::memcpy(h.data(), &head, sizeof(head));
+  std::memcpy(h.data() + d3s::LB_ARGS_OFF, args.data(), args.size() * sizeof(d3s::Args));
+  std::memcpy(h.data() + d3s::lb_rows_off(n_domains), rows.data(), rows.size() * sizeof(int2));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemcpyAsync(desc, h.data(), h.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(e, "links batch: descriptor upload");
+  *work_ints = d3s::LB_HEAD + 3 * capacity;
+  std::lock_guard<std::mutex> lk(d3s::g_lb_mu);
+  d3s::g_lb[desc] = {n_domains, int(rows.size()), max_box, *work_ints, worlds[0].storage.dtype};
+  return HL_OK;
+}
+
+extern "C" int hl_d3q27_solid_links_batch(const void* desc, int n_domains, int parity, int32_t* work, size_t work_ints,
+                                          hl_stream stream) {
+  HL_CHECK_ARG(desc != nullptr && work != nullptr, "links batch: descriptors or work list is NULL");
+  HL_CHECK_ARG(parity == 0 || parity == 1, "links batch: parity %d", parity);
+  d3s::BatchInfo b;
+  {
+    std::lock_guard<std::mutex> lk(d3s::g_lb_mu);
+    auto it = d3s::g_lb.find(desc);
+    HL_CHECK_ARG(it != d3s::g_lb.end() && it->second.n_domains == n_domains,
+                 "links batch: descriptors not prepared for %d domains", n_domains);
+    b = it->second;
+  }
+  HL_CHECK_ARG(work_ints >= b.work_ints, "links batch: work list of %zu ints (needs %zu)", work_ints, b.work_ints);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(work, 0, d3s::LB_HEAD * sizeof(int32_t), st);
+  if (e != cudaSuccess) return cuda_status(e, "links batch: zero work counters");
+  switch (b.dtype) {
+    case HL_F32: return d3s::launch_batch<StoreF32>(desc, b, parity, work, st);
+    case HL_F16: return d3s::launch_batch<StoreF16>(desc, b, parity, work, st);
+    case HL_BF16: return d3s::launch_batch<StoreBF16>(desc, b, parity, work, st);
+    case HL_F64: return d3s::launch_batch<StoreF64>(desc, b, parity, work, st);
+  }
+  set_error("links batch: storage dtype %d not supported", int(b.dtype));
+  return HL_ERR_UNSUPPORTED;
 }

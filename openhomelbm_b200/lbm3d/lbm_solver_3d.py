@@ -189,12 +189,13 @@ class LBM_Solver3D:
         return any(t is not None and len(t) for t in self._mesh_tris)
 
     # ------------------------------------------------------------------ stepping
-    def _launch(self, parity: int, stream, loads_out=None, stream_collide: bool = True) -> None:
+    def _launch(self, parity: int, stream, loads_out=None, stream_collide: bool = True,
+                solid_links: bool = True) -> None:
         """One step of every world on ``stream``. ``loads_out`` (optional, per world a pair of
         device pointers) redirects the binary32 solid force / torque [n][3] of the step.
-        ``stream_collide=False`` leaves out the stream-collide launch (a batched launch over
-        several solvers' worlds, hl_d3q27_stream_collide_batch, does it) and enqueues only the
-        cut links and the boundaries that follow it."""
+        ``stream_collide=False`` / ``solid_links=False`` leave out the stream-collide / cut-link
+        launches (batched launches over several solvers' worlds, hl_d3q27_stream_collide_batch
+        and hl_d3q27_solid_links_batch, do them); the boundaries always follow."""
         L = _lib.lib()
         meshes = self.has_meshes
         for k, f in enumerate(self.flows):
@@ -205,7 +206,7 @@ class LBM_Solver3D:
                                     self.mass[k:k + 1].data_ptr(), self.health[k:k + 1].data_ptr())
             if stream_collide:
                 _lib.check(L.hl_d3q27_stream_collide(w, float(f.vis_shear), diag, stream), "stream_and_collide_3d")
-            if meshes:
+            if meshes and solid_links:
                 sst = self._solids_struct(k)
                 if loads_out is not None:
                     sst.force, sst.torque = loads_out[k]

@@ -11,8 +11,9 @@ domain's whole control step (pose updates, stream-collide, cut links, boundaries
 copies for all substeps) is captured once into a CUDA graph at admission and each tick
 launches every active domain's graph on its own CUDA stream, so the domains' kernels overlap
 on the device. With ``batched=True`` each substep is instead ONE stream-collide launch over
-every active domain (hl_d3q27_stream_collide_batch: the tiles of all domains share the SMs),
-then each domain's cut links, boundaries, load copy and next pose on its own stream; once the
+every active domain (hl_d3q27_stream_collide_batch: the tiles of all domains share the SMs)
+and ONE cut-link pass over all of them (hl_d3q27_solid_links_batch), then each domain's
+boundaries and next pose on its own stream; once the
 set of active domains has held for two ticks, the whole control step of the set is one CUDA
 graph (``TickGraph``). Both give the same results; the batched form's stream-collide is
 faster, but its cut links and boundaries then run between two batched launches instead of
@@ -34,7 +35,7 @@ import math
 import os
 import time
 from dataclasses import dataclass, field
-from typing import Dict, List, Tuple
+from typing import Dict, List, Optional, Tuple
 
 import numpy as np
 import torch
@@ -218,8 +219,8 @@ class Domain:
             if self.batched:
                 self.pre_graph = self._capture(lambda: self._pose(0))
                 S = req.substeps
-                self.post_graphs = [self._capture(lambda k=k: self._after_stream_collide(k, k + 1 < S))
-                                    for k in range(S)]
+                # what follows the batched stream-collide and cut links of substep k
+                self.post_graphs = [self._capture(lambda k=k: self._after_links(k, k + 1 < S)) for k in range(S)]
             else:
                 self.graph = self._capture(self._control_step)
         self.event = torch.cuda.Event()
@@ -248,6 +249,13 @@ class Domain:
         """Substep k after its stream-collide: cut links (loads into slot k), boundaries, and the
         pose of substep k + 1."""
         self.solver._launch(k % 2, _lib.stream_ptr(), loads_out=self._loads_out(k), stream_collide=False)
+        if next_pose:
+            self._pose(k + 1)
+
+    def _after_links(self, k: int, next_pose: bool) -> None:
+        """Substep k after its batched stream-collide and cut links: boundaries and the pose of
+        substep k + 1."""
+        self.solver._launch(k % 2, _lib.stream_ptr(), stream_collide=False, solid_links=False)
         if next_pose:
             self._pose(k + 1)
 
@@ -356,15 +364,56 @@ class BatchStep:
             self.status.data_ptr(), _lib.stream_ptr(stream)), "batched stream-collide")
 
 
+class LinkBatch:
+    """The cut links of a set of domains in one classify and one process launch
+    (hl_d3q27_solid_links_batch). Each substep writes its loads into its own slot of every
+    domain's load buffer, so there is one descriptor set per substep."""
+
+    def __init__(self, domains: List[Domain], stream: torch.cuda.Stream):
+        L = _lib.lib()
+        flows = [d.solver.flows[0] for d in domains]
+        self.vis = float(flows[0].vis_shear)
+        self.n = len(domains)
+        total = sum(int(d.solver.solid_num) for d in domains)
+        nbytes = int(L.hl_d3q27_links_batch_bytes(self.n, total))
+        dev = flows[0].device
+        self.descs = []
+        need = 0
+        for k in range(domains[0].req.substeps):
+            worlds = (_lib.hl_world3d * self.n)(*[f.world_struct(0) for f in flows])
+            structs = []
+            for d in domains:
+                sst = d.solver._solids_struct(0)
+                sst.force, sst.torque = d._loads_out(k)[0]
+                structs.append(sst)
+            solids = (_lib.hl_solids3d * self.n)(*structs)
+            buf = torch.empty(nbytes + 64, dtype=torch.uint8, device=dev)
+            ptr = (buf.data_ptr() + 63) // 64 * 64
+            wi = ctypes.c_size_t(0)
+            _lib.check(L.hl_d3q27_links_batch_prepare(worlds, solids, self.n, self.vis, ptr, nbytes, ctypes.byref(wi),
+                                                      _lib.stream_ptr(stream)), "batched cut links (prepare)")
+            self.descs.append((buf, ptr))
+            need = max(need, int(wi.value))
+        self.work = torch.zeros(max(need, 1), dtype=torch.int32, device=dev)
+
+    def launch(self, k: int, stream: torch.cuda.Stream) -> None:
+        """The cut links of substep k (parity k % 2), loads into slot k."""
+        _lib.check(_lib.lib().hl_d3q27_solid_links_batch(
+            self.descs[k][1], self.n, k % 2, self.work.data_ptr(), self.work.numel(), _lib.stream_ptr(stream)),
+            "batched cut links")
+
+
 class TickGraph:
     """One control step of a fixed set of batched domains as ONE CUDA graph: the pose of
-    substep 0 of every domain, then per substep the batched stream-collide followed by every
-    domain's cut links, boundaries, load copy and next pose, each domain on its own branch.
+    substep 0 of every domain, then per substep the batched stream-collide and cut links (the
+    latter per domain when ``links`` is None) followed by every domain's boundaries and next
+    pose, each domain on its own branch.
     Replaying it costs the host one launch instead of a few calls per domain and substep (which
     leave the device idle between substeps). The pose upload and load download stay outside, on
     the replaying stream."""
 
-    def __init__(self, domains: List[Domain], batch: "BatchStep", main: torch.cuda.Stream):
+    def __init__(self, domains: List[Domain], batch: "BatchStep", main: torch.cuda.Stream,
+                 links: Optional[LinkBatch] = None):
         S = domains[0].req.substeps
         torch.cuda.synchronize()
         fork = torch.cuda.Event()
@@ -382,11 +431,16 @@ class TickGraph:
                 for rd in ready:
                     main.wait_event(rd[k])
                 batch.launch(k % 2, main)
+                if links is not None:
+                    links.launch(k, main)
                 sc_done[k].record(main)
                 for d, rd in zip(domains, ready):
                     d.stream.wait_event(sc_done[k])
                     with torch.cuda.stream(d.stream):
-                        d._after_stream_collide(k, k + 1 < S)
+                        if links is not None:
+                            d._after_links(k, k + 1 < S)
+                        else:
+                            d._after_stream_collide(k, k + 1 < S)
                     rd[k + 1].record(d.stream)
             for rd in ready:
                 main.wait_event(rd[S])
@@ -455,7 +509,7 @@ class ServeEngine:
         main = torch.cuda.Stream(device=self.device)
         sc_done = torch.cuda.Event()
         tick_done = torch.cuda.Event()
-        batch, batch_ids, tick_graph, stable = None, None, None, 0
+        batch, links, batch_ids, tick_graph, stable = None, None, None, None, 0
         while pending or active:
             admit()
             if not active:
@@ -466,6 +520,7 @@ class ServeEngine:
             if self.batched:
                 if batch_ids != [id(d) for d in running]:
                     batch = BatchStep(running, main)  # the set changed: new descriptors
+                    links = LinkBatch(running, main)
                     batch_ids = [id(d) for d in running]
                     tick_graph, stable = None, 0
                 else:
@@ -473,7 +528,7 @@ class ServeEngine:
                 # one graph per set, once the set has held for two ticks (while domains arrive
                 # or finish every tick, capturing would cost more than it saves)
                 if tick_graph is None and stable >= 2:
-                    tick_graph = TickGraph(running, batch, main)
+                    tick_graph = TickGraph(running, batch, main, links)
             t0 = time.perf_counter()
             if tick_graph is not None:
                 with torch.cuda.stream(main):
@@ -492,6 +547,7 @@ class ServeEngine:
                     for d in running:
                         main.wait_event(d.ready)
                     batch.launch(k % 2, main)
+                    links.launch(k, main)
                     sc_done.record(main)
                     for d in running:
                         d.after(k, sc_done)

@@ -107,3 +107,45 @@ def test_batch_rejects_bad_arguments():
                                                    _lib.stream_ptr()))
     with pytest.raises(ValueError):
         Domain(Request(0, 64, 1, 0.0, control_steps=1, substeps=3), "float16", 0.01, torch.device("cuda:0"))
+
+
+def test_batched_cut_links_equal_per_domain():
+    """hl_d3q27_solid_links_batch over three served domains computes, between the same
+    stream-collide and boundary launches, exactly the moments the per-domain cut links compute;
+    the loads agree to binary32 rounding (binary64 sums in another order)."""
+    from openhomelbm_b200 import _lib
+    from openhomelbm_b200.serving import Domain, LinkBatch, Request
+
+    doms = [Domain(Request(k, side, 31 + k, 0.0, control_steps=4, substeps=2), "float16", 0.01,
+                   torch.device("cuda:0"), use_graph=False) for k, side in enumerate((64, 96, 128))]
+    for step in range(2):  # swimmers moving, a developed flow
+        for d in doms:
+            d.stage_poses(step)
+            d.launch()
+        for d in doms:
+            d.event.synchronize()
+            d.finish(0.0)
+    L = _lib.lib()
+    st = _lib.stream_ptr()
+    links = LinkBatch(doms, torch.cuda.current_stream())
+    ref = []
+    for d in doms:
+        f = d.solver.flows[0]
+        f.moments[1].zero_()
+        d.solver._launch(0, st, loads_out=d._loads_out(0))
+        torch.cuda.synchronize()
+        ref.append((f.moments[1].clone(), d.loads_dev[0].clone()))
+    for d in doms:
+        f = d.solver.flows[0]
+        f.moments[1].zero_()
+        d.loads_dev.zero_()
+        _lib.check(L.hl_d3q27_stream_collide(f.world_struct(0), float(f.vis_shear), None, st), "stream-collide")
+    links.launch(0, torch.cuda.current_stream())
+    for d in doms:
+        d.solver._launch(0, st, stream_collide=False, solid_links=False)
+    torch.cuda.synchronize()
+    for d, (m, loads) in zip(doms, ref):
+        assert torch.equal(d.solver.flows[0].moments[1], m), d.req.side
+        a, b = d.loads_dev[0].double(), loads.double()
+        assert b.abs().max() > 0
+        assert (a - b).abs().max() <= 1e-6 * b.abs().max(), d.req.side
