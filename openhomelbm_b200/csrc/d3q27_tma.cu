@@ -222,8 +222,11 @@ template <class S> __device__ __forceinline__ void encode_pair(const Mom3<P2>& m
 // Raw planes of one cell of a staged plane (k-th moment plane at p[k * stride]). A cell
 // outside a walled domain must read as the zero cell. The TMA unit zero-fills boxes outside
 // the tensor, which IS the zero cell of float32 storage (rho = 0, drho = -1); the encoded
-// storages store rho - 1 and need the select (SEL). A lane past the last source plane of an
-// item holds stale data: its populations only reach destinations that are never stored.
+// storages store rho - 1 and need the select (SEL) where an outside cell can feed a stored
+// one: with a flag array (a border cell may be fluid). Without one, only the interior cells
+// are stored and all their neighbours lie inside, so what an outside cell sends reaches only
+// border cells, which are never stored. A lane past the last source plane of an item holds
+// stale data: its populations only reach destinations that are never stored.
 template <class S, bool SEL>
 __device__ __forceinline__ void load_raw(const typename S::T* p0, const typename S::T* p1, int stride, bool in0,
                                          bool in1, P2 raw[10]) {
@@ -247,7 +250,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   using T = typename S::T;
   static_assert(sizeof(typename S::R) == 4, "the paired kernel computes in binary32");
   using G = Geo<T, NSTAGE>;
-  constexpr bool SEL = S::kEncoded && !PERIODIC;  // see load_raw
+  constexpr bool SEL = S::kEncoded && !PERIODIC && FLAGS;  // see load_raw
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + G::BAR_OFF);
