@@ -58,9 +58,12 @@ def profile_traffic(n, storage):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """nvidia-smi clocks and throttle reasons around the timed region, every 100 ms, each
+    sample with nvidia-smi's own timestamp (the pipe delivers lines in bursts). The caller keeps
+    the GPU loaded before and after the timed steps, so that a timed region shorter than the
+    sampling period still has a sample under load on each side."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -73,7 +76,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
@@ -93,25 +96,42 @@ class ClockSampler:
                 self.proc.kill()
         return False
 
-    def summary(self):
-        sm, mx, reasons = [], [], set()
+    def samples(self):
+        """(unix time, sm MHz, max sm MHz, set of active reasons) per parsed line."""
+        import datetime
+
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in self.lines:
+        out = []
+        for ln in list(self.lines):
             parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx.append(float(parts[2]))
+                t = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                sm, mx = float(parts[2]), float(parts[3])
             except ValueError:
                 continue
-            for name, val in zip(names, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(name)
-        if not sm:
+            out.append((t, sm, mx, {n for n, v in zip(names, parts[6:10]) if v.lower().startswith("active")}))
+        return out
+
+    def seen_after(self, t: float) -> bool:
+        return any(s[0] >= t for s in self.samples())
+
+    def summary(self, t_open: float, t_close: float):
+        """The samples inside [t_open, t_close]; if the region was shorter than the sampling
+        period, the nearest loaded sample on each side of it."""
+        ss = self.samples()
+        inside = [s for s in ss if t_open <= s[0] <= t_close]
+        window = "timed region"
+        if not inside:
+            before = [s for s in ss if s[0] < t_open][-1:]
+            after = [s for s in ss if s[0] > t_close][:1]
+            inside, window = before + after, "nearest sample on each side (timed region shorter than the 100 ms period)"
+        if not inside:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = set().union(*(s[3] for s in inside))
+        return {"sm_mhz": float(np.median([s[1] for s in inside])), "sm_max_mhz": float(max(s[2] for s in inside)),
+                "reasons": sorted(reasons), "samples": len(inside), "window": window}
 
 
 def cpu_baseline(n_yz, budget_s=12.0, nthreads=0):
@@ -219,17 +239,31 @@ def run_ours(args, rank, world, dist):
         torch.cuda.synchronize()
 
     # ---------------------------------------------------------------- device-resident timing
-    for _ in range(max(args.warmup, 3)):
-        s.step()
-    barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev.index) as clk:
+        # warm-up: at least W steps, continued (at most 5 s) until the clock sampler has
+        # logged the GPU under this load
+        t_warm = time.time()
+        done = 0
+        while done < max(args.warmup, 3) or (clk.proc is not None and time.time() - t_warm < 5.0 and
+                                             (done % 32 or not clk.seen_after(t_warm + 0.15))):
+            s.step()
+            done += 1
+            if done % 64 == 0:
+                torch.cuda.synchronize()
         barrier()
+        t_open = time.time()
         start.record(stream)
         for _ in range(args.steps):
             s.step()
         end.record(stream)
         barrier()
+        t_close = time.time()
+        # keep the load (untimed) for one sampling period, so a sample follows the region
+        while time.time() - t_close < 0.15:
+            s.step()
+            torch.cuda.synchronize()
+        time.sleep(0.15)
     ms = start.elapsed_time(end)
     if dist is not None:
         t = torch.tensor([ms], device=dev)
@@ -295,9 +329,10 @@ def run_ours(args, rank, world, dist):
                         "each step's mass and health words copied to pinned host memory and awaited by the "
                         "host, final field downloaded; host wall clock"},
         "gpu_launches": args.steps * (1 + (0 if f.periodic else 3)),
+        "warmup_steps_run": done,
         "health_nonfinite_cells": health,
     }
-    c = clk.summary()
+    c = clk.summary(t_open, t_close)
     if c is not None:
         out["clocks"] = c
     if world == 1 and not args.no_cpu_baseline:
