@@ -169,6 +169,38 @@ def cpu_baseline(n_yz, budget_s=12.0, nthreads=0):
 
 
 # ----------------------------------------------------------------------------- arms
+# ----------------------------------------------------------------------------- replicas
+def init_replicas(backend: str = "nccl", timeout_s: float = 300.0):
+    """(rank, world, torch.distributed or None) from the launcher's RANK / WORLD_SIZE /
+    MASTER_* environment; one process per GPU, each stepping its own replica."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world <= 1:
+        return rank, world, None
+    import datetime
+
+    import torch.distributed as tdist
+
+    tdist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=timeout_s))
+    return rank, world, tdist
+
+
+def max_over_ranks(x: float, dist, device=None) -> float:
+    """The largest x over the ranks (the slowest replica's time); x itself without a group."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, cells_per_replica: int, steps: int, seconds: float) -> float:
+    """Whole-job MLUPS: every replica's cell updates over the slowest replica's time."""
+    return world * cells_per_replica * steps / seconds / 1e6
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return None
@@ -264,13 +296,9 @@ def run_ours(args, rank, world, dist):
             s.step()
             torch.cuda.synchronize()
         time.sleep(0.15)
-    ms = start.elapsed_time(end)
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(start.elapsed_time(end), dist, dev)
     ms_step = ms / args.steps
-    value = world * cells * args.steps / (ms / 1e3) / 1e6
+    value = job_rate(world, cells, args.steps, ms / 1e3)
 
     # ---------------------------------------------------------------- end to end, host buffers
     # Through the public API (LBM_Solver3D.step -> libhomelbm): the job's input field is
@@ -294,12 +322,8 @@ def run_ours(args, rank, world, dist):
         stream.synchronize()
     out_host.copy_(f.cur, non_blocking=True)
     stream.synchronize()
-    e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_s = float(t.item())
-    e2e = world * cells * ke / e_s / 1e6
+    e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    e2e = job_rate(world, cells, ke, e_s)
     field_bytes = init_host.numel() * init_host.element_size()
     health = int(health_host.max().item())
     s.diagnostics = False
@@ -679,14 +703,10 @@ def main():
     if world > 1 and args.impl == "reference" and rank != 0:
         return  # the CPU arm runs on rank 0 only
     if world > 1 and args.impl != "reference":
-        import datetime
-
         import torch
-        import torch.distributed as tdist
 
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-        tdist.init_process_group(backend="nccl", timeout=datetime.timedelta(seconds=300))
-        dist = tdist
+        rank, world, dist = init_replicas("nccl")
     try:
         if args.impl == "reference":
             out = run_reference(args, rank, world)
