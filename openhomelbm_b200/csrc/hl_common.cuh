@@ -79,19 +79,27 @@ inline Scale make_scale(const hl_storage& st) {
 __device__ __forceinline__ unsigned dither_bits(unsigned b, unsigned salt) {
   return (b ^ (salt * 0x9e3779b9u)) * 0x85ebca6bu;
 }
+// The same kind of hash for the moments of one cell stored together: the value's bits, the
+// cell's term cell_salt = cell index * 0x9e3779b9 (taken once per cell) and moment k's own
+// constant (folded at compile time) -- one three-way xor and one multiply per element.
+__device__ __forceinline__ unsigned dither_cell(unsigned b, unsigned cell_salt, unsigned k) {
+  return (b ^ cell_salt ^ (k * 0x632be5abu)) * 0x85ebca6bu;
+}
 // binary32 -> binary16, stochastic. Normal range: add 13 random bits below the binary16 unit
 // of the last place to the magnitude and truncate. Below the smallest normal (2^-14) the
 // spacing is the fixed 2^-24: floor(v 2^24 + U), U uniform in [0, 1), then exact.
-__device__ __forceinline__ __half half_sr(float v, unsigned salt) {
+__device__ __forceinline__ __half half_sr_bits(float v, unsigned h, bool keep_nonfinite) {
   const unsigned b = __float_as_uint(v);
-  const unsigned h = dither_bits(b, salt);
   if (fabsf(v) < 6.103515625e-05f) {
     const float q = v * 16777216.f;                        // exact
     const float u = float(h >> 8) * (1.0f / 16777216.f);   // [0, 1)
     return __float2half_rn(floorf(q + u) * 5.9604644775390625e-08f);
   }
-  const unsigned r = (b & 0x7f800000u) == 0x7f800000u ? 0u : h >> 19;  // inf, nan unchanged
+  const unsigned r = keep_nonfinite && (b & 0x7f800000u) == 0x7f800000u ? 0u : h >> 19;  // inf, nan unchanged
   return __float2half_rz(__uint_as_float(b + r));
+}
+__device__ __forceinline__ __half half_sr(float v, unsigned salt) {
+  return half_sr_bits(v, dither_bits(__float_as_uint(v), salt), true);
 }
 // binary32 -> bfloat16, stochastic: 16 random bits below the bfloat16 unit of the last place
 // (same exponent range as binary32, so no subnormal case short of binary32's own).
@@ -107,6 +115,7 @@ struct StoreF32 {
   static constexpr bool kEncoded = false;
   __device__ static float to_r(T v) { return v; }
   __device__ static T from_r(float v, unsigned = 0u) { return v; }
+  __device__ static T from_r_cell(float v, unsigned, unsigned) { return v; }
 };
 struct StoreF64 {
   using T = double;
@@ -114,6 +123,7 @@ struct StoreF64 {
   static constexpr bool kEncoded = false;
   __device__ static double to_r(T v) { return v; }
   __device__ static T from_r(double v, unsigned = 0u) { return v; }
+  __device__ static T from_r_cell(double v, unsigned, unsigned) { return v; }
 };
 struct StoreF16 {
   using T = __half;
@@ -122,6 +132,11 @@ struct StoreF16 {
   __device__ static float to_r(T v) { return __half2float(v); }
   // salt: the element's index in its buffer
   __device__ static T from_r(float v, unsigned salt = 0u) { return half_sr(v, salt); }
+  // moment k of the cell whose cell_salt is given (dither_cell); a non-finite value stays
+  // non-finite (an infinity may come out as a NaN)
+  __device__ static T from_r_cell(float v, unsigned cell_salt, unsigned k) {
+    return half_sr_bits(v, dither_cell(__float_as_uint(v), cell_salt, k), false);
+  }
 };
 struct StoreBF16 {
   using T = __nv_bfloat16;
@@ -129,6 +144,10 @@ struct StoreBF16 {
   static constexpr bool kEncoded = true;
   __device__ static float to_r(T v) { return __bfloat162float(v); }
   __device__ static T from_r(float v, unsigned salt = 0u) { return bf16_sr(v, salt); }
+  __device__ static T from_r_cell(float v, unsigned cell_salt, unsigned k) {
+    const unsigned b = __float_as_uint(v);
+    return __float2bfloat16_rz(__uint_as_float(b + (dither_cell(b, cell_salt, k) >> 16)));
+  }
 };
 
 // raw[10] in plane order -> physical moments
