@@ -179,8 +179,11 @@ template <class S> __device__ __forceinline__ void store2(const World& w, long l
                                                           const Mom2<typename S::R>& v) {
   typename S::R raw[6];
   encode2<S>(v, w.sc, raw);
+  // stochastic rounding of the reduced storages: one hash term per cell (dither_cell), the
+  // same in every D2Q9 kernel so that they store a cell identically
+  const unsigned cs = unsigned(i) * 0x9e3779b9u;
 #pragma unroll
-  for (int k = 0; k < 6; ++k) m[k * N + i] = S::from_r(raw[k], unsigned(k * N + i));
+  for (int k = 0; k < 6; ++k) m[k * N + i] = S::from_r_cell(raw[k], cs, unsigned(k));
 }
 
 __device__ __forceinline__ bool is_fluid(const World& w, int x, int y, long long i) {
@@ -381,8 +384,9 @@ __global__ void __launch_bounds__(TILE_THREADS) stream_tiles_kernel(const __grid
       const R Fx = fxp ? R(fxp[ci]) : R(0), Fy = fyp ? R(fyp[ci]) : R(0);
       R raw[6];
       encode2<S>(collide<R>(pop, Fx, Fy, omega), sc, raw);
+      const unsigned cs = unsigned(ci) * 0x9e3779b9u;  // as store2
 #pragma unroll
-      for (int k = 0; k < 6; ++k) post[k * N + ci] = S::from_r(raw[k], unsigned(k * N + ci));
+      for (int k = 0; k < 6; ++k) post[k * N + ci] = S::from_r_cell(raw[k], cs, unsigned(k));
     }
   }
 }
