@@ -305,7 +305,7 @@ def run_ours(args, rank, world, dist):
     # uploaded from pinned host memory inside the timed region, every step's result (the
     # binary64 mass and the health word) is copied to pinned host memory and waited for by
     # the host before the next step, and the final field is downloaded at the end.
-    ke = min(args.steps, args.e2e_steps)
+    ke = args.steps if args.e2e_steps <= 0 else min(args.steps, args.e2e_steps)  # default: the same K steps
     init_host = f.cur.detach().to("cpu").pin_memory()
     out_host = torch.empty_like(init_host).pin_memory()
     mass_host = torch.empty(ke, dtype=torch.float64).pin_memory()
@@ -672,7 +672,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end run (0: --steps)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--storage", default="float32", choices=list(BYTES_PER_CELL))
