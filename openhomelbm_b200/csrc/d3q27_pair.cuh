@@ -153,7 +153,9 @@ __device__ __forceinline__ void rebuild_face(const Coef& c, const PairConst& k, 
 template <bool FORCE>
 __device__ __forceinline__ Mom3<P2> collide_pair(const Acc<P2>& a, P2 Fx, P2 Fy, P2 Fz, const PairConst& k) {
   const P2 rho = a.rho + P2(1.f, 1.f);
-  // 1 / rho: hardware estimate, then one Newton step r + r (1 - rho r) on both lanes
+  // 1 / rho: the rcp.approx estimate (relative error below 2^-22 by the PTX ISA), then one
+  // Newton-Raphson step for f(r) = 1/r - rho, r <- r + r (1 - rho r), which squares the relative
+  // error to the binary32 rounding level; the parity tests against the binary64 oracle bound it
   const P2 r0(rcp_approx(rho.x()), rcp_approx(rho.y()));
   const P2 inv = r0 * (P2(1.f, 1.f) - rho * r0) + r0;
   P2 ux, uy, uz;
