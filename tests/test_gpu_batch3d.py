@@ -30,7 +30,7 @@ def _solver(nx, ny, nz, storage, seed):
     return s
 
 
-@pytest.mark.parametrize("storage", ["float32", "float16"])
+@pytest.mark.parametrize("storage", ["float32", "float16", "bfloat16"])
 def test_batched_stream_collide_equals_one_launch_per_domain(storage):
     from openhomelbm_b200 import _lib
     from openhomelbm_b200.serving import BatchStep
@@ -109,14 +109,15 @@ def test_batch_rejects_bad_arguments():
         Domain(Request(0, 64, 1, 0.0, control_steps=1, substeps=3), "float16", 0.01, torch.device("cuda:0"))
 
 
-def test_batched_cut_links_equal_per_domain():
+@pytest.mark.parametrize("storage", ["float16", "float32", "bfloat16"])
+def test_batched_cut_links_equal_per_domain(storage):
     """hl_d3q27_solid_links_batch over three served domains computes, between the same
     stream-collide and boundary launches, exactly the moments the per-domain cut links compute;
     the loads agree to binary32 rounding (binary64 sums in another order)."""
     from openhomelbm_b200 import _lib
     from openhomelbm_b200.serving import Domain, LinkBatch, Request
 
-    doms = [Domain(Request(k, side, 31 + k, 0.0, control_steps=4, substeps=2), "float16", 0.01,
+    doms = [Domain(Request(k, side, 31 + k, 0.0, control_steps=4, substeps=2), storage, 0.01,
                    torch.device("cuda:0"), use_graph=False) for k, side in enumerate((64, 96, 128))]
     for step in range(2):  # swimmers moving, a developed flow
         for d in doms:
