@@ -33,3 +33,45 @@ def test_argument_errors_are_reported_without_touching_the_gpu():
     w2.nx, w2.ny = 8, 8
     rc = lib.hl_d2q9_step(ctypes.byref(w2), ctypes.byref(_lib.hl_step2d(0.1, 0.0, 0.0)), None, None, None)
     assert rc == _lib.HL_ERR_ARG
+
+
+def test_batch_live_view_and_control_arguments_are_checked_without_the_gpu():
+    """The batched, live-view and 2D control entry points reject bad arguments before any CUDA
+    call: NULL buffers, empty batches, misaligned or unprepared descriptors, bad axes."""
+    lib = _lib.load()
+    arg = _lib.HL_ERR_ARG
+    w = _lib.hl_world3d()
+    w.nx, w.ny, w.nz = 16, 16, 16
+    worlds = (_lib.hl_world3d * 1)(w)
+    n = ctypes.c_int(0)
+    assert lib.hl_d3q27_batch_bytes(0) == 0
+    assert lib.hl_d3q27_batch_prepare(worlds, 0, 64, 1 << 20, ctypes.byref(n), None) == arg
+    assert lib.hl_d3q27_batch_prepare(worlds, 1, 64 + 16, 1 << 20, ctypes.byref(n), None) == arg
+    assert b"64-byte" in lib.hl_last_error()
+    assert lib.hl_d3q27_batch_prepare(worlds, 1, 64, 8, ctypes.byref(n), None) == arg
+    assert b"too small" in lib.hl_last_error()
+    stor = _lib.hl_storage()
+    assert lib.hl_d3q27_stream_collide_batch(4096, 1, 1, 0.02, ctypes.byref(stor), 0, None, None) == arg
+    assert lib.hl_d3q27_stream_collide_batch(4096, 1, 1, 0.02, ctypes.byref(stor), 2, None, None) == arg
+    assert lib.hl_d3q27_links_batch_bytes(0, 3) == 0
+    solids = (_lib.hl_solids3d * 1)()
+    work = ctypes.c_size_t(0)
+    assert lib.hl_d3q27_links_batch_prepare(worlds, solids, 0, 0.02, 64, 1 << 20, ctypes.byref(work), None) == arg
+    assert lib.hl_d3q27_links_batch_prepare(worlds, solids, 1, 0.02, 64, 1 << 20, ctypes.byref(work), None) == arg
+    assert b"world" in lib.hl_last_error()  # the domain's buffers are NULL
+    assert lib.hl_d3q27_solid_links_batch(64, 1, 3, 64, 1 << 20, None) == arg
+    assert lib.hl_d3q27_solid_links_batch(64, 1, 0, 64, 1 << 20, None) == arg
+    assert b"not prepared" in lib.hl_last_error()
+    pos = (ctypes.c_int32 * 1)(3)
+    assert lib.hl_d3q27_live_slices(ctypes.byref(w), pos, 1, 8, 8, 1, 0, 0, 0, 0, 64, None, None) == arg  # cur NULL
+    w.cur = 64
+    assert lib.hl_d3q27_live_slices(ctypes.byref(w), pos, 1, 8, 8, 1, 3, 0, 0, 0, 64, None, None) == arg
+    assert b"axis" in lib.hl_last_error()
+    assert lib.hl_d3q27_live_slices(ctypes.byref(w), pos, 1, 8, 8, 1, 0, 0, 0, 1, 64, None, None) == arg
+    assert b"histogram" in lib.hl_last_error()
+    assert lib.hl_live_rgba(None, 0, 1.0, 1.0, None, None) == _lib.HL_OK  # nothing to colour
+    assert lib.hl_live_rgba(None, 4, 1.0, 1.0, None, None) == arg
+    assert lib.hl_d2q9_uimg_rgba(64, 8, 8, 3, 1.0, 64, None) == arg
+    assert b"render mode" in lib.hl_last_error()
+    assert lib.hl_d2q9_local_force(None, None, 8, 8, 1.0, 1.0, 1.0, 1.0, 0.1, 0.0, None) == arg
+    assert lib.hl_d2q9_local_force(64, 64, 0, 8, 1.0, 1.0, 1.0, 1.0, 0.1, 0.0, None) == arg
