@@ -75,6 +75,17 @@ typedef struct {
   float s_scale; /* scale of S - u u */
 } hl_storage;
 
+/* Round already-encoded binary32 moments into a storage type exactly as the stream-collide
+ * kernels store them. values and out are [n_moments][n_cells] (plane order); cell c's moment
+ * k is stored as moment k of cell first_cell + c. HL_F16 / HL_BF16 round stochastically (a
+ * value goes to the upper neighbour with probability equal to its distance from the lower
+ * one, the random bits a hash of the value, the cell and k); paired != 0 rounds cells 2j and
+ * 2j + 1 in one two-lane conversion, as the TMA kernel does, with the same results. HL_F32
+ * copies, HL_F64 widens. An extension: the reference stores binary32 only (HomeFlow3D's
+ * fields are wp.float32, envs/lbm3d/lbm_core_3d.py:66-82). */
+HL_API int hl_round_to_storage(const float* values, long long n_cells, int n_moments, hl_dtype dtype,
+                               long long first_cell, int paired, void* out, hl_stream stream);
+
 /* ------------------------------------------------------------------ D3Q27 */
 /* One D3Q27 world. cur/post are the two moment buffers (the reference's fields and their
  * *_post twins); the step reads cur and writes post, and the caller swaps them afterwards

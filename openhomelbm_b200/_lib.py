@@ -86,6 +86,7 @@ _SIGS = {
     "hl_d3q27_live_slices": ([POINTER(hl_world3d), c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int,
                               c_void_p, c_void_p, c_void_p], c_int),
     "hl_live_rgba": ([c_void_p, c_longlong, c_float, c_float, c_void_p, c_void_p], c_int),
+    "hl_round_to_storage": ([c_void_p, c_longlong, c_int, c_int, c_longlong, c_int, c_void_p, c_void_p], c_int),
     "hl_d2q9_uimg_rgba": ([c_void_p, c_int, c_int, c_int, c_float, c_void_p, c_void_p], c_int),
     "hl_d2q9_local_force": ([c_void_p, c_void_p, c_int, c_int, c_float, c_float, c_float, c_float, c_float, c_float,
                              c_void_p], c_int),

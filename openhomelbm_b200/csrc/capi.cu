@@ -55,3 +55,60 @@ extern "C" int hl_set_tuning(const char* key, int value) {
   hl::set_error("hl_set_tuning: unknown key or value (%s = %d)", key, value);
   return HL_ERR_ARG;
 }
+
+namespace hl {
+namespace {
+
+// one thread per cell (per pair of cells when paired), every moment of it
+template <class S>
+__global__ void round_to_storage_kernel(const float* __restrict__ v, long long n, int nm, long long first, bool paired,
+                                        typename S::T* __restrict__ out) {
+  using T = typename S::T;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long c = paired ? 2 * t : t;
+  if (c >= n) return;
+  const unsigned cs0 = unsigned(first + c) * 0x9e3779b9u;
+  if (paired && c + 1 < n) {
+    const unsigned cs1 = unsigned(first + c + 1) * 0x9e3779b9u;
+    for (int k = 0; k < nm; ++k) {
+      T a, b;
+      S::from_r_cell2(v[k * n + c], v[k * n + c + 1], cs0, cs1, unsigned(k), a, b);
+      out[k * n + c] = a;
+      out[k * n + c + 1] = b;
+    }
+  } else {
+    for (int k = 0; k < nm; ++k) out[k * n + c] = S::from_r_cell(v[k * n + c], cs0, unsigned(k));
+  }
+}
+
+template <class S>
+int launch_round(const float* v, long long n, int nm, long long first, bool paired, void* out, cudaStream_t st) {
+  const long long threads = paired ? (n + 1) / 2 : n;
+  round_to_storage_kernel<S><<<unsigned((threads + 255) / 256), 256, 0, st>>>(v, n, nm, first, paired,
+                                                                              static_cast<typename S::T*>(out));
+  HL_LAUNCH_CHECK("round to storage");
+  return HL_OK;
+}
+
+}  // namespace
+}  // namespace hl
+
+extern "C" int hl_round_to_storage(const float* values, long long n_cells, int n_moments, hl_dtype dtype,
+                                   long long first_cell, int paired, void* out, hl_stream stream) {
+  using namespace hl;
+  HL_CHECK_ARG(n_cells >= 0 && n_cells < (1ll << 38) && n_moments >= 1 && n_moments <= 64,
+               "round to storage: %lld cells of %d moments", n_cells, n_moments);
+  HL_CHECK_ARG(n_cells == 0 || (values != nullptr && out != nullptr), "round to storage: values or out is NULL");
+  HL_CHECK_ARG(first_cell >= 0, "round to storage: negative first cell");
+  if (n_cells == 0) return HL_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const bool p = paired != 0;
+  switch (dtype) {
+    case HL_F32: return launch_round<StoreF32>(values, n_cells, n_moments, first_cell, p, out, st);
+    case HL_F16: return launch_round<StoreF16>(values, n_cells, n_moments, first_cell, p, out, st);
+    case HL_BF16: return launch_round<StoreBF16>(values, n_cells, n_moments, first_cell, p, out, st);
+    case HL_F64: return launch_round<StoreF64>(values, n_cells, n_moments, first_cell, p, out, st);
+  }
+  set_error("round to storage: dtype %d", int(dtype));
+  return HL_ERR_ARG;
+}

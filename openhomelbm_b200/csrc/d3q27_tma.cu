@@ -566,13 +566,27 @@ __global__ void __launch_bounds__(THREADS, 1)
           encode_pair<S>(m, a.sc, raw);
           // stochastic rounding of the reduced storages: one salt term per cell (dither_cell)
           const unsigned cs0 = unsigned(c0) * 0x9e3779b9u, cs1 = unsigned(c1) * 0x9e3779b9u;
-          if (f0) {
+          if constexpr (S::kEncoded) {  // both cells' moment k in one conversion, packed
+            unsigned d[10];
 #pragma unroll
-            for (int k = 0; k < 10; ++k) post[k * N + c0] = S::from_r_cell(raw[k].x(), cs0, unsigned(k));
-          }
-          if (f1) {
+            for (int k = 0; k < 10; ++k) d[k] = S::round2(raw[k].x(), raw[k].y(), cs0, cs1, unsigned(k));
+            if (f0) {
 #pragma unroll
-            for (int k = 0; k < 10; ++k) post[k * N + c1] = S::from_r_cell(raw[k].y(), cs1, unsigned(k));
+              for (int k = 0; k < 10; ++k) post[k * N + c0] = S::hi(d[k]);
+            }
+            if (f1) {
+#pragma unroll
+              for (int k = 0; k < 10; ++k) post[k * N + c1] = S::lo(d[k]);
+            }
+          } else {
+            if (f0) {
+#pragma unroll
+              for (int k = 0; k < 10; ++k) post[k * N + c0] = S::from_r_cell(raw[k].x(), cs0, unsigned(k));
+            }
+            if (f1) {
+#pragma unroll
+              for (int k = 0; k < 10; ++k) post[k * N + c1] = S::from_r_cell(raw[k].y(), cs1, unsigned(k));
+            }
           }
           if (DIAG) {
             const P2 s = m.ux + m.uy + m.uz + m.sxx + m.syy + m.szz + m.sxy + m.sxz + m.syz;

@@ -69,13 +69,14 @@ inline Scale make_scale(const hl_storage& st) {
 // goes to the upper one with probability equal to its distance from the lower one, in units
 // of their spacing (unbiased in expectation). Round-to-nearest stores of a slowly varying
 // field round the same way step after step and its error drifts; stochastic rounding makes
-// the per-step errors independent. The random bits are the top bits of a multiplicative hash
+// the per-step errors independent. The random bits are bits of a multiplicative hash
 // (Knuth's multiplicative hashing, golden-ratio and MurmurHash3-finaliser constants) of the
 // value's own bit pattern and a salt (the element's index in its buffer): a store is a
 // deterministic function of the value and its place, so a field gives the same result in
 // every run, alone or batched, while equal values in different cells round independently.
-// The top bits of the product depend on every input bit, the dropped low bits included, and
-// are uniform over the values and places a field holds, which is what unbiasedness needs.
+// Bits 16 and up of the product depend on every input bit below them, the dropped low bits of
+// the value included, and are uniform over the values and places a field holds, which is what
+// unbiasedness needs.
 __device__ __forceinline__ unsigned dither_bits(unsigned b, unsigned salt) {
   return (b ^ (salt * 0x9e3779b9u)) * 0x85ebca6bu;
 }
@@ -85,28 +86,43 @@ __device__ __forceinline__ unsigned dither_bits(unsigned b, unsigned salt) {
 __device__ __forceinline__ unsigned dither_cell(unsigned b, unsigned cell_salt, unsigned k) {
   return (b ^ cell_salt ^ (k * 0x632be5abu)) * 0x85ebca6bu;
 }
-// binary32 -> binary16, stochastic. Normal range: add 13 random bits below the binary16 unit
-// of the last place to the magnitude and truncate. Below the smallest normal (2^-14) the
-// spacing is the fixed 2^-24: floor(v 2^24 + U), U uniform in [0, 1), then exact.
-__device__ __forceinline__ __half half_sr_bits(float v, unsigned h, bool keep_nonfinite) {
-  const unsigned b = __float_as_uint(v);
-  if (fabsf(v) < 6.103515625e-05f) {
-    const float q = v * 16777216.f;                        // exact
-    const float u = float(h >> 8) * (1.0f / 16777216.f);   // [0, 1)
-    return __float2half_rn(floorf(q + u) * 5.9604644775390625e-08f);
-  }
-  const unsigned r = keep_nonfinite && (b & 0x7f800000u) == 0x7f800000u ? 0u : h >> 19;  // inf, nan unchanged
-  return __float2half_rz(__uint_as_float(b + r));
+// The rounding itself is the sm_100a conversion with caller-supplied random bits
+// (cvt.rs.{f16x2,bf16x2}.f32): a goes to the upper half of the result and b to the lower one.
+// binary16: a draws its 13 random bits from rbits[28:16], b from rbits[12:0]; they are added
+// below the unit of the last place and the sum is truncated, the subnormal range (spacing
+// 2^-24) included, where the fraction is first cut to 13 bits (a bias toward zero under
+// 2^-37). bfloat16: 16 random bits each, a from rbits[31:16], b from rbits[15:0]. Finite
+// values above the largest finite one round to it or to an infinity; infinities and NaNs
+// stay non-finite. The probability and the bit fields are checked on the GPU by the rounding test
+// of the storage codecs (hl_round_to_storage).
+__device__ __forceinline__ unsigned cvt_rs_f16x2(float a, float b, unsigned rbits) {
+  unsigned d;
+  asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(a), "f"(b), "r"(rbits));
+  return d;
 }
+__device__ __forceinline__ unsigned cvt_rs_bf16x2(float a, float b, unsigned rbits) {
+  unsigned d;
+  asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(a), "f"(b), "r"(rbits));
+  return d;
+}
+// rbits for a pair whose hashes are ha (value a) and hb (value b): bits 31..16 of ha in the
+// upper half, bits 31..16 of hb in the lower half, so that a and b round exactly as they
+// would alone (the single forms put a value in the a slot with its hash as rbits).
+__device__ __forceinline__ unsigned pair_rbits(unsigned ha, unsigned hb) { return __byte_perm(ha, hb, 0x3276u); }
+__device__ __forceinline__ __half half_hi(unsigned d) { return __ushort_as_half((unsigned short)(d >> 16)); }
+__device__ __forceinline__ __half half_lo(unsigned d) { return __ushort_as_half((unsigned short)(d & 0xffffu)); }
+__device__ __forceinline__ __nv_bfloat16 bf16_hi(unsigned d) {
+  return __ushort_as_bfloat16((unsigned short)(d >> 16));
+}
+__device__ __forceinline__ __nv_bfloat16 bf16_lo(unsigned d) {
+  return __ushort_as_bfloat16((unsigned short)(d & 0xffffu));
+}
+// binary32 -> binary16 / bfloat16, stochastic, with the element-index salt
 __device__ __forceinline__ __half half_sr(float v, unsigned salt) {
-  return half_sr_bits(v, dither_bits(__float_as_uint(v), salt), true);
+  return half_hi(cvt_rs_f16x2(v, 0.f, dither_bits(__float_as_uint(v), salt)));
 }
-// binary32 -> bfloat16, stochastic: 16 random bits below the bfloat16 unit of the last place
-// (same exponent range as binary32, so no subnormal case short of binary32's own).
 __device__ __forceinline__ __nv_bfloat16 bf16_sr(float v, unsigned salt) {
-  const unsigned b = __float_as_uint(v);
-  const unsigned r = (b & 0x7f800000u) == 0x7f800000u ? 0u : dither_bits(b, salt) >> 16;  // inf, nan unchanged
-  return __float2bfloat16_rz(__uint_as_float(b + r));
+  return bf16_hi(cvt_rs_bf16x2(v, 0.f, dither_bits(__float_as_uint(v), salt)));
 }
 
 struct StoreF32 {
@@ -116,6 +132,10 @@ struct StoreF32 {
   __device__ static float to_r(T v) { return v; }
   __device__ static T from_r(float v, unsigned = 0u) { return v; }
   __device__ static T from_r_cell(float v, unsigned, unsigned) { return v; }
+  __device__ static void from_r_cell2(float a, float b, unsigned, unsigned, unsigned, T& oa, T& ob) {
+    oa = a;
+    ob = b;
+  }
 };
 struct StoreF64 {
   using T = double;
@@ -124,6 +144,10 @@ struct StoreF64 {
   __device__ static double to_r(T v) { return v; }
   __device__ static T from_r(double v, unsigned = 0u) { return v; }
   __device__ static T from_r_cell(double v, unsigned, unsigned) { return v; }
+  __device__ static void from_r_cell2(double a, double b, unsigned, unsigned, unsigned, T& oa, T& ob) {
+    oa = a;
+    ob = b;
+  }
 };
 struct StoreF16 {
   using T = __half;
@@ -132,10 +156,22 @@ struct StoreF16 {
   __device__ static float to_r(T v) { return __half2float(v); }
   // salt: the element's index in its buffer
   __device__ static T from_r(float v, unsigned salt = 0u) { return half_sr(v, salt); }
-  // moment k of the cell whose cell_salt is given (dither_cell); a non-finite value stays
-  // non-finite (an infinity may come out as a NaN)
+  // moment k of the cell whose cell_salt is given (dither_cell)
   __device__ static T from_r_cell(float v, unsigned cell_salt, unsigned k) {
-    return half_sr_bits(v, dither_cell(__float_as_uint(v), cell_salt, k), false);
+    return half_hi(cvt_rs_f16x2(v, 0.f, dither_cell(__float_as_uint(v), cell_salt, k)));
+  }
+  // moment k of two cells at once, packed (a in the upper half): the same results as two
+  // from_r_cell calls, one conversion
+  __device__ static unsigned round2(float a, float b, unsigned cs_a, unsigned cs_b, unsigned k) {
+    return cvt_rs_f16x2(a, b, pair_rbits(dither_cell(__float_as_uint(a), cs_a, k),
+                                         dither_cell(__float_as_uint(b), cs_b, k)));
+  }
+  __device__ static T hi(unsigned d) { return half_hi(d); }
+  __device__ static T lo(unsigned d) { return half_lo(d); }
+  __device__ static void from_r_cell2(float a, float b, unsigned cs_a, unsigned cs_b, unsigned k, T& oa, T& ob) {
+    const unsigned d = round2(a, b, cs_a, cs_b, k);
+    oa = hi(d);
+    ob = lo(d);
   }
 };
 struct StoreBF16 {
@@ -145,8 +181,18 @@ struct StoreBF16 {
   __device__ static float to_r(T v) { return __bfloat162float(v); }
   __device__ static T from_r(float v, unsigned salt = 0u) { return bf16_sr(v, salt); }
   __device__ static T from_r_cell(float v, unsigned cell_salt, unsigned k) {
-    const unsigned b = __float_as_uint(v);
-    return __float2bfloat16_rz(__uint_as_float(b + (dither_cell(b, cell_salt, k) >> 16)));
+    return bf16_hi(cvt_rs_bf16x2(v, 0.f, dither_cell(__float_as_uint(v), cell_salt, k)));
+  }
+  __device__ static unsigned round2(float a, float b, unsigned cs_a, unsigned cs_b, unsigned k) {
+    return cvt_rs_bf16x2(a, b, pair_rbits(dither_cell(__float_as_uint(a), cs_a, k),
+                                          dither_cell(__float_as_uint(b), cs_b, k)));
+  }
+  __device__ static T hi(unsigned d) { return bf16_hi(d); }
+  __device__ static T lo(unsigned d) { return bf16_lo(d); }
+  __device__ static void from_r_cell2(float a, float b, unsigned cs_a, unsigned cs_b, unsigned k, T& oa, T& ob) {
+    const unsigned d = round2(a, b, cs_a, cs_b, k);
+    oa = hi(d);
+    ob = lo(d);
   }
 };
 

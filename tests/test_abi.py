@@ -75,3 +75,14 @@ def test_batch_live_view_and_control_arguments_are_checked_without_the_gpu():
     assert b"render mode" in lib.hl_last_error()
     assert lib.hl_d2q9_local_force(None, None, 8, 8, 1.0, 1.0, 1.0, 1.0, 0.1, 0.0, None) == arg
     assert lib.hl_d2q9_local_force(64, 64, 0, 8, 1.0, 1.0, 1.0, 1.0, 0.1, 0.0, None) == arg
+
+
+def test_round_to_storage_arguments_are_checked_without_the_gpu():
+    lib = _lib.load()
+    arg = _lib.HL_ERR_ARG
+    assert lib.hl_round_to_storage(None, 0, 10, 1, 0, 0, None, None) == _lib.HL_OK  # nothing to round
+    assert lib.hl_round_to_storage(None, 4, 10, 1, 0, 0, None, None) == arg
+    assert lib.hl_round_to_storage(64, 4, 0, 1, 0, 0, 64, None) == arg
+    assert lib.hl_round_to_storage(64, 4, 10, 1, -1, 0, 64, None) == arg
+    assert lib.hl_round_to_storage(64, 4, 10, 9, 0, 0, 64, None) == arg
+    assert b"dtype" in lib.hl_last_error()
