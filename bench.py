@@ -561,7 +561,8 @@ def run_serve(args):
     serving.ServeEngine(storage="float16", max_active=1).run(warm, realtime=False)
     torch.cuda.synchronize()
     plain = serving.run_plain(reqs, storage="float32")
-    served = serving.ServeEngine(storage="float16", max_active=args.slots, budget_bytes=150e9).run(reqs)
+    engine = serving.ServeEngine(storage="float16", max_active=args.slots, budget_bytes=150e9)
+    served = engine.run(reqs)
     # the same requests with one stream-collide launch per substep over all active domains
     batched = serving.ServeEngine(storage="float16", max_active=args.slots, budget_bytes=150e9,
                                   batched=True).run(reqs)
@@ -599,7 +600,7 @@ def run_serve(args):
             "u_l2_f16_vs_f64_by_side": u_l2,
             "u_l2_f16_vs_f64": {"median": float(np.median(all_e)), "max": float(np.max(all_e))},
             "config": {"requests": len(reqs), "rate_per_s": args.rate, "control_steps": args.control_steps,
-                       "substeps": 8, "slots": args.slots, "hbm_budget_gb": 150,
+                       "substeps": 8, "slots": args.slots, "hbm_budget_gb": 150, "served_x_chunks": engine.x_chunks,
                        "sides": {str(k): sides.count(k) for k in sorted(set(sides))},
                        "triangles_per_body": 1800, "segments": serving.SEGMENTS}}
 

@@ -58,7 +58,8 @@ HL_API const char* hl_version(void);
 
 /* Process-wide tuning knobs (no reference counterpart; for benchmarking and tests):
  *   "d3q27_kernel": 0 automatic, 1 the asynchronous-copy kernel, 2 the TMA-staged kernel
- *   "d3q27_chunks": 0 automatic, k > 0 splits x into k chunks per tile column
+ *   "d3q27_chunks": 0 automatic, k > 0 splits x into k chunks per tile column (read by
+ *     hl_d3q27_stream_collide at launch and by hl_d3q27_batch_prepare)
  *   "d3q27_stages": 0 automatic (4), 3..5 planes staged by the TMA kernel
  *   "d3q27_link_blocks": 0 automatic (4 per SM), k > 0 blocks of the cut-link kernel over the
  *     listed cells (fewer leave SMs free for other domains' kernels on other streams)

@@ -203,6 +203,15 @@ def torch_dtype(code: int):
     return {HL_F32: torch.float32, HL_F16: torch.float16, HL_BF16: torch.bfloat16, HL_F64: torch.float64}[code]
 
 
+_TUNING: dict = {}
+
+
 def set_tuning(key: str, value: int) -> None:
     """hl_set_tuning: process-wide kernel selection / work split knobs (see homelbm.h)."""
     check(lib().hl_set_tuning(key.encode(), int(value)), "hl_set_tuning")
+    _TUNING[key] = int(value)
+
+
+def get_tuning(key: str) -> int:
+    """The value last set through set_tuning (0, the library's automatic choice, if never set)."""
+    return _TUNING.get(key, 0)

@@ -896,9 +896,10 @@ extern "C" int hl_d3q27_batch_prepare(const hl_world3d* worlds, int n_domains, v
     d.nz = w.nz;
     d.tiles_z = w.nz / d3::tma::TZ;
     d.n_tiles = (w.ny / d3::tma::TY) * d.tiles_z;
-    // x chunks of about 32 planes: with the items of every domain to spread over the SMs,
-    // the chunks only need to be long against the two halo planes each one reads
-    const int chunks = std::max(1, (w.nx + 16) / 32);
+    // x chunks of about 32 planes (or the "d3q27_chunks" override): with the items of every
+    // domain to spread over the SMs, the chunks only need to be long against the two halo
+    // planes each one reads
+    const int chunks = g_tune_d3_chunks > 0 ? std::min(g_tune_d3_chunks, w.nx) : std::max(1, (w.nx + 16) / 32);
     d.chunk_len = (w.nx + chunks - 1) / chunks;
     d.n_items = d.n_tiles * ((w.nx + d.chunk_len - 1) / d.chunk_len);
     d.item_base = int(total);
