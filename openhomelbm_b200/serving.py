@@ -536,24 +536,34 @@ class ServeEngine:
         def now():
             return time.perf_counter() - t_start
 
-        def admit():
+        prepared: List[Domain] = []  # admitted, built while the device ran a tick, not yet stepped
+
+        def build(limit: int) -> List[Domain]:
+            """Domains for up to ``limit`` pending requests (arrived, within the HBM budget)."""
             nonlocal used
-            while pending and len(active) < self.max_active and (not realtime or pending[0].arrival <= now()):
+            out = []
+            while len(out) < limit and pending and (not realtime or pending[0].arrival <= now()):
                 need = domain_bytes(pending[0].side, self.storage)
                 if used + need > self.budget:
                     break
                 r = pending.pop(0)
                 d = Domain(r, self.storage, self.vis, self.device, batched=self.batched)
                 d.stage_poses(0)
-                active.append(d)
+                out.append(d)
                 used += need
                 order.append(r.rid)
+            return out
+
+        def admit():
+            while prepared and len(active) < self.max_active:
+                active.append(prepared.pop(0))
+            active.extend(build(self.max_active - len(active)))
 
         main = torch.cuda.Stream(device=self.device)
         sc_done = torch.cuda.Event()
         tick_done = torch.cuda.Event()
         batch, links, batch_ids, tick_graph, stable = None, None, None, None, 0
-        while pending or active:
+        while pending or active or prepared:
             admit()
             if not active:
                 time.sleep(max(0.0, min(pending[0].arrival - now(), 0.01)))
@@ -599,10 +609,20 @@ class ServeEngine:
             else:
                 for d in running:
                     d.launch()
-            # while the device works: the poses of every domain's next control step
+            # while the device works: the poses of every domain's next control step, and the
+            # domains of the requests that take the slots freed after this tick (a domain costs
+            # ~8 ms of host time to build, which otherwise leaves the device idle), one at a time
+            # and only while the tick is still running, so that the tick's latency stays its own
             for d in running:
                 if d.done + 1 < d.req.control_steps:
                     d.stage_poses(d.done + 1)
+            want = self.max_active - len(active) + sum(1 for d in running if d.done + 1 >= d.req.control_steps)
+            while len(prepared) < want and not (tick_done.query() if tick_graph is not None
+                                                else all(d.event.query() for d in running)):
+                got = build(1)
+                if not got:
+                    break
+                prepared.extend(got)
             if tick_graph is not None:
                 tick_done.synchronize()
             else:
