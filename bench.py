@@ -601,6 +601,7 @@ def run_serve(args):
             "u_l2_f16_vs_f64": {"median": float(np.median(all_e)), "max": float(np.max(all_e))},
             "config": {"requests": len(reqs), "rate_per_s": args.rate, "control_steps": args.control_steps,
                        "substeps": 8, "slots": args.slots, "hbm_budget_gb": 150, "served_x_chunks": engine.x_chunks,
+                       "served_link_blocks": engine.link_blocks,
                        "sides": {str(k): sides.count(k) for k in sorted(set(sides))},
                        "triangles_per_body": 1800, "segments": serving.SEGMENTS}}
 

@@ -489,7 +489,7 @@ class ServeEngine:
 
     def __init__(self, storage: str = "float16", budget_bytes: float = 150e9, max_active: int = 32,
                  vis: float = 0.01, device=None, keep_fields: bool = False, batched: bool = False,
-                 x_chunks: Optional[int] = None):
+                 x_chunks: Optional[int] = None, link_blocks: Optional[int] = None):
         self.storage = storage
         self.budget = float(budget_bytes)
         self.max_active = int(max_active)
@@ -514,15 +514,27 @@ class ServeEngine:
         self.x_chunks = int(x_chunks)
         if self.x_chunks < 0:
             raise ValueError(f"x_chunks must be >= 0, got {x_chunks}")
+        # blocks of each domain's cut-link kernel (the library's "d3q27_link_blocks" while run()
+        # lasts; 0 keeps the library's 4 per SM). None: one per SM for per-domain graphs, 0 for
+        # the batched form. With resident domains sharing the GPU, one block per SM left the
+        # other domains' kernels more room: control-step p50 21.65-21.70 ms at 148-296 blocks
+        # against 22.0 ms at the automatic 592 (and 23.0 ms at 37).
+        if link_blocks is None:
+            link_blocks = 0 if self.batched else torch.cuda.get_device_properties(self.device).multi_processor_count
+        self.link_blocks = int(link_blocks)
+        if not 0 <= self.link_blocks <= 4096:
+            raise ValueError(f"link_blocks must be in 0..4096, got {link_blocks}")
 
     def run(self, requests: List[Request], realtime: bool = True) -> ServeStats:
         """Serve the requests (arrival times honoured when ``realtime``) until all finish."""
-        prev = _lib.get_tuning("d3q27_chunks")
+        prev = {k: _lib.get_tuning(k) for k in ("d3q27_chunks", "d3q27_link_blocks")}
         _lib.set_tuning("d3q27_chunks", self.x_chunks)
+        _lib.set_tuning("d3q27_link_blocks", self.link_blocks)
         try:
             return self._run(requests, realtime)
         finally:
-            _lib.set_tuning("d3q27_chunks", prev)
+            for k, v in prev.items():
+                _lib.set_tuning(k, v)
 
     def _run(self, requests: List[Request], realtime: bool) -> ServeStats:
         pending = sorted(requests, key=lambda r: r.arrival)

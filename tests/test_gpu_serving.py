@@ -62,20 +62,25 @@ def test_admission_respects_slots_and_budget():
 
 @pytest.mark.parametrize("batched", [False, True])
 def test_x_split_of_served_domains_does_not_change_results(batched):
-    """ServeEngine(x_chunks=k) runs its domains' stream-collide with k x chunks per tile column
-    (0: the library's automatic split) and restores the process-wide setting afterwards; the
-    split changes which CTA computes a plane, not what it computes."""
+    """ServeEngine(x_chunks=k, link_blocks=b) runs its domains' stream-collide with k x chunks
+    per tile column and their cut links on b blocks (0: the library's automatic choices) and
+    restores the process-wide settings afterwards; the split and the grid change which CTA
+    computes a plane or a cell, not what it computes."""
     from openhomelbm_b200 import _lib
     from openhomelbm_b200.serving import ServeEngine
 
     reqs = _reqs()
     _lib.set_tuning("d3q27_chunks", 0)
-    runs = {k: ServeEngine(storage="float16", max_active=3, batched=batched, x_chunks=k, keep_fields=True)
-            .run(reqs, realtime=False) for k in (0, 1, 3)}
-    assert _lib.get_tuning("d3q27_chunks") == 0
+    _lib.set_tuning("d3q27_link_blocks", 0)
+    blocks = {0: 0, 1: 148, 3: 37}  # the cut-link grid changes which block takes a cell, too
+    runs = {k: ServeEngine(storage="float16", max_active=3, batched=batched, x_chunks=k, link_blocks=blocks[k],
+                           keep_fields=True).run(reqs, realtime=False) for k in (0, 1, 3)}
+    assert _lib.get_tuning("d3q27_chunks") == 0 and _lib.get_tuning("d3q27_link_blocks") == 0
     for k in (1, 3):
         for r in reqs:
             np.testing.assert_array_equal(runs[k].fields[r.rid], runs[0].fields[r.rid])
             assert _close(runs[k].results[r.rid], runs[0].results[r.rid])
     with pytest.raises(ValueError):
         ServeEngine(x_chunks=-1)
+    with pytest.raises(ValueError):
+        ServeEngine(link_blocks=-1)
