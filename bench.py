@@ -134,38 +134,67 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(inside), "window": window}
 
 
-def cpu_baseline(n_yz, budget_s=12.0, nthreads=0):
-    """The oracle (C++ restatement of the reference kernels, all host threads) on a periodic
-    slab of the workload's cross-section; returns MLUPS and the sample description."""
-    from oracle import oracle as orc
+CPU_SLAB_PLANES = 8  # x planes of the periodic slab both CPU legs time
 
-    threads = nthreads or orc.max_threads()
-    nx = 8
-    u0 = 0.04
-    x = 2 * np.pi * np.arange(n_yz) / n_yz
+
+def tgv_slab(n, nx, u0=0.04):
+    """The first nx x planes of the n^3 Taylor-Green initial state (float32 moments), as a
+    periodic slab: the CPU legs time the same per-cell work on a bounded sample."""
+    x = 2 * np.pi * np.arange(n) / n
     Y, Z = np.meshgrid(x, x, indexing="ij")
-    X = (2 * np.pi * np.arange(nx) / n_yz)[:, None, None]
+    X = (2 * np.pi * np.arange(nx) / n)[:, None, None]
     ux = u0 * np.sin(X) * np.cos(Y) * np.cos(Z)
     uy = -u0 * np.cos(X) * np.sin(Y) * np.cos(Z)
     uz = np.zeros_like(ux)
     rho = 1 + 3 * (u0 ** 2 / 16) * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2)
-    m = np.stack([rho, ux, uy, uz, ux * ux, uy * uy, uz * uz, ux * uy, ux * uz, uy * uz]).astype(np.float32)
-    prev = m.copy()
-    vis = np.float32(u0 * (n_yz / (2 * np.pi)) / 1600.0)
-    orc.step_3d(m, prev, vis_shear=vis, periodic=True, nthreads=threads)  # warm-up
+    return np.stack([rho, ux, uy, uz, ux * ux, uy * uy, uz * uz, ux * uy, ux * uz, uy * uz]).astype(np.float32)
+
+
+class CpuSlab:
+    """The oracle (C++ restatement of the reference's stream_and_collide_3d) stepping a periodic
+    slab of the workload on every host thread. The oracle splits a step over (x, y) rows, so
+    each of the threads gets work (2048 rows at 256^2)."""
+
+    def __init__(self, n, nx=CPU_SLAB_PLANES, u0=0.04):
+        from oracle import oracle as orc
+
+        self.orc = orc
+        self.threads = orc.max_threads()
+        self.n, self.nx = n, nx
+        self.m = tgv_slab(n, nx, u0)
+        self.prev = self.m.copy()
+        self.vis = np.float32(u0 * (n / (2 * np.pi)) / 1600.0)
+        self.cells = nx * n * n
+
+    @property
+    def cores(self):
+        return min(self.threads, self.nx * self.n)
+
+    def step(self):
+        new, _ = self.orc.step_3d(self.m, self.prev, vis_shear=self.vis, periodic=True, nthreads=self.threads)
+        self.m, self.prev = new, self.m
+
+    def sample(self):
+        return (f"one stream-collide per step of a periodic {self.nx}x{self.n}x{self.n} slab of the {self.n}^3 "
+                f"workload on {self.cores} host threads split over (x, y) rows (C++ restatement of the reference's "
+                f"stream_and_collide_3d; Warp is not installable here)")
+
+
+def cpu_baseline(n_yz, budget_s=12.0):
+    """The oracle on a periodic slab of the workload for about budget_s seconds; MLUPS and the
+    sample description."""
+    slab = CpuSlab(n_yz)
+    slab.step()  # warm-up
     steps = 0
     t0 = time.perf_counter()
     while True:
-        new, _ = orc.step_3d(m, prev, vis_shear=vis, periodic=True, nthreads=threads)
-        m, prev = new, m
+        slab.step()
         steps += 1
         if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
-    cells = nx * n_yz * n_yz
-    return {"value": cells * steps / dt / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{steps} steps of a periodic {nx}x{n_yz}x{n_yz} slab of the workload "
-                      f"({dt:.1f} s, C++ restatement of stream_and_collide_3d, not Warp)"}
+    return {"value": slab.cells * steps / dt / 1e6, "unit": UNIT, "cores": slab.cores, "kind": "port",
+            "sample": f"{steps} steps ({dt:.1f} s): " + slab.sample()}
 
 
 # ----------------------------------------------------------------------------- arms
@@ -204,41 +233,23 @@ def job_rate(world: int, cells_per_replica: int, steps: int, seconds: float) -> 
 def run_reference(args, rank, world):
     if rank != 0:
         return None
-    from oracle import oracle as orc
-
-    threads = orc.max_threads()
     n = args.n
-    nx = 4
-    u0 = 0.04
-    x = 2 * np.pi * np.arange(n) / n
-    Y, Z = np.meshgrid(x, x, indexing="ij")
-    X = (2 * np.pi * np.arange(nx) / n)[:, None, None]
-    ux = u0 * np.sin(X) * np.cos(Y) * np.cos(Z)
-    uy = -u0 * np.cos(X) * np.sin(Y) * np.cos(Z)
-    z0 = np.zeros_like(ux)
-    rho = 1 + 3 * (u0 ** 2 / 16) * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2)
-    m = np.stack([rho, ux, uy, z0, ux * ux, uy * uy, z0, ux * uy, z0, z0]).astype(np.float32)
-    prev = m.copy()
-    vis = np.float32(u0 * (n / (2 * np.pi)) / 1600.0)
+    slab = CpuSlab(n)
     for _ in range(args.warmup):
-        new, _ = orc.step_3d(m, prev, vis_shear=vis, periodic=True, nthreads=threads)
-        m, prev = new, m
+        slab.step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        new, _ = orc.step_3d(m, prev, vis_shear=vis, periodic=True, nthreads=threads)
-        m, prev = new, m
+        slab.step()
     dt = time.perf_counter() - t0
-    cells = nx * n * n
-    value = cells * args.steps / dt / 1e6
-    sample = (f"each step is one stream-collide of a periodic {nx}x{n}x{n} slab of the {n}^3 workload "
-              f"(C++ restatement of the reference's stream_and_collide_3d; Warp is not installable here)")
+    value = slab.cells * args.steps / dt / 1e6
     return {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (Taylor-Green initial state)",
-            "config": {"workload": f"D3Q27 Taylor-Green vortex {n}^3 periodic, FP32", "u0": u0,
-                       "Re": 1600, "sample_cells": cells},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "config": {"workload": f"D3Q27 Taylor-Green vortex {n}^3 periodic, FP32", "u0": 0.04,
+                       "Re": 1600, "sample_cells": slab.cells},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": slab.cores, "kind": "port",
+                             "sample": slab.sample()},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -544,7 +555,7 @@ def run_karman(args):
 
 
 # ----------------------------------------------------------------------------- serving form
-def run_serve(args):
+def run_serve(args, batched_variant=True):
     """The serving form: Poisson arrivals of mesh-coupled D3Q27 domains (sides log-uniform in
     64-192, rounded to multiples of 32; a 5-segment swimmer of 1800 triangles; 8 LBM substeps
     per control step, 100 control steps per request). The served engine (float16 storage,
@@ -564,8 +575,8 @@ def run_serve(args):
     engine = serving.ServeEngine(storage="float16", max_active=args.slots, budget_bytes=150e9)
     served = engine.run(reqs)
     # the same requests with one stream-collide launch per substep over all active domains
-    batched = serving.ServeEngine(storage="float16", max_active=args.slots, budget_bytes=150e9,
-                                  batched=True).run(reqs)
+    batched = (serving.ServeEngine(storage="float16", max_active=args.slots, budget_bytes=150e9,
+                                   batched=True).run(reqs) if batched_variant else None)
     # agreement of the served float16 loads with the plain float32 loads, request by request
     errs = []
     for r in reqs:
@@ -592,8 +603,9 @@ def run_serve(args):
                        "p99_ms": served.pct(99) * 1e3, "p99_over_p50": served.pct(99) / served.pct(50),
                        "wall_s": served.wall_s, "max_active": served.max_active,
                        "mlups": cells / served.wall_s / 1e6},
-            "served_batched_stream_collide": {"env_steps_per_s": batched.env_steps_per_s,
-                                              "p50_ms": batched.pct(50) * 1e3, "p99_ms": batched.pct(99) * 1e3},
+            "served_batched_stream_collide": ({"env_steps_per_s": batched.env_steps_per_s,
+                                               "p50_ms": batched.pct(50) * 1e3, "p99_ms": batched.pct(99) * 1e3}
+                                              if batched is not None else None),
             "plain": {"env_steps_per_s": plain.env_steps_per_s, "p50_ms": plain.pct(50) * 1e3,
                       "p99_ms": plain.pct(99) * 1e3, "wall_s": plain.wall_s, "mlups": cells / plain.wall_s / 1e6},
             "loads_rel_l2_f16_vs_plain_f32": {"median": float(np.median(errs)), "max": float(np.max(errs))},
@@ -669,6 +681,27 @@ def run_batch(args):
                        "l2": "inputs larger than L2"}}
 
 
+def serve_leg(args):
+    """The serving form's figures for the default line: served (float16, continuous batching)
+    against the plain float32 solver one request at a time, on the same seeded requests."""
+    r = run_serve(args, batched_variant=False)
+    keep = ("env_steps_per_s", "p50_ms", "p99_ms", "p99_over_p50", "wall_s", "max_active")
+    return {"metric": r["metric"], "value": r["value"], "unit": r["unit"], "vs_plain": r["vs_plain"],
+            "served": {k: r["served"][k] for k in keep},
+            "plain": {k: r["plain"][k] for k in ("env_steps_per_s", "p50_ms", "p99_ms", "wall_s")},
+            "u_l2_f16_vs_f64": r["u_l2_f16_vs_f64"], "loads_rel_l2_f16_vs_plain_f32": r["loads_rel_l2_f16_vs_plain_f32"],
+            "config": r["config"]}
+
+
+def batch_leg(args):
+    """The batching form's figures for the default line: 64 uneven D2Q9 worlds in one persistent
+    launch per substep, against the same worlds solved one at a time."""
+    r = run_batch(args)
+    return {"metric": r["metric"], "value": r["value"], "unit": r["unit"], "vs_sequential": r["vs_sequential"],
+            "batched": r["batched"], "sequential_plain": r["sequential_plain"], "roofline": r["roofline"],
+            "loads_rel_l2_f16_batch_vs_plain_f32": r["loads_rel_l2_f16_batch_vs_plain_f32"], "config": r["config"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -695,8 +728,12 @@ def main():
     ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate (requests/s)")
     ap.add_argument("--control-steps", type=int, default=100, help="serve: control steps per request")
     ap.add_argument("--slots", type=int, default=32, help="serve: concurrently resident domains")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="tgv: leave out the serve and batch legs of the default line")
     args = ap.parse_args()
-    if args.workload == "serve":
+    legs = args.workload == "tgv" and args.impl == "ours" and not args.no_legs and \
+        int(os.environ.get("WORLD_SIZE", "1")) == 1
+    if args.workload == "serve" or legs:
         # a hardware work queue per resident domain's stream (before any CUDA call)
         os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -722,6 +759,15 @@ def main():
             out = run_batch(args) if rank == 0 else None
         else:
             out = run_ours(args, rank, world, dist)
+            if legs and out is not None:
+                # the second half of the headline metric (served env-steps/s and latency against
+                # the plain solver) and the batching form, measured in the same run
+                t0 = time.perf_counter()
+                out["serve"] = serve_leg(args)
+                out["serve"]["leg_wall_s"] = time.perf_counter() - t0
+                t0 = time.perf_counter()
+                out["batch"] = batch_leg(args)
+                out["batch"]["leg_wall_s"] = time.perf_counter() - t0
         if rank == 0 and out is not None:
             print(json.dumps(out), flush=True)
     finally:

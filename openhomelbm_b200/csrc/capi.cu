@@ -5,6 +5,9 @@
 #include "hl_common.cuh"
 
 #include <cstring>
+#include <mutex>
+#include <set>
+#include <tuple>
 
 namespace hl {
 
@@ -24,6 +27,33 @@ void set_error(const char* fmt, ...) {
 int cuda_status(cudaError_t e, const char* what) {
   set_error("%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
   return HL_ERR_CUDA;
+}
+
+int device_sms() {
+  constexpr int kMaxDev = 128;
+  static int cache[kMaxDev] = {};  // 0: not queried yet (written once per device, int-sized)
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 148;
+  if (dev < kMaxDev && __atomic_load_n(&cache[dev], __ATOMIC_ACQUIRE) > 0) return cache[dev];
+  int n = 0;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  if (dev < kMaxDev) __atomic_store_n(&cache[dev], n, __ATOMIC_RELEASE);
+  return n;
+}
+
+int set_smem_attr(const void* kernel, int bytes, const char* what) {
+  static std::mutex mu;
+  static std::set<std::tuple<const void*, int, int>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e, what);
+  const auto key = std::make_tuple(kernel, dev, bytes);
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count(key)) return HL_OK;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return cuda_status(e, what);
+  done.insert(key);
+  return HL_OK;
 }
 
 }  // namespace hl

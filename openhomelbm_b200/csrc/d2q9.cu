@@ -810,8 +810,8 @@ template <class S, int TX, int TY> int launch_tiles(const d2::Launch& L, const T
   auto kern = d2::stream_tiles_kernel<S, TX, TY>;
   const size_t smem = d2::tile_smem_bytes<TX, TY, typename S::R>();
   if (smem > 48 * 1024) {
-    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return cuda_status(e, "d2q9 tiles: shared memory size");
+    const int rc = set_smem_attr(reinterpret_cast<const void*>(kern), int(smem), "d2q9 tiles: shared memory size");
+    if (rc != HL_OK) return rc;
   }
   const int grid = tw.n_tiles < tw.ctas ? tw.n_tiles : tw.ctas;
   kern<<<grid, d2::TILE_THREADS, smem, st>>>(L, tw.tiles, tw.n_tiles);

@@ -226,16 +226,7 @@ template <int TY, class S> size_t smem_bytes() {
   return st + 27 * TL::NSRC * sizeof(typename S::R);
 }
 
-int num_sms() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
-  return n;
-}
+int num_sms() { return device_sms(); }
 
 // Work split: tiles x x-chunks. All CTAs march whole x ranges in step so that halo reloads
 // are L2 hits; x is split only when that fills the SMs with less waste.
@@ -303,12 +294,8 @@ int launch_step(const hl_world3d* w, double vis_shear, const hl_diag* diag, cuda
   if (DIAG) fill_diag(a, diag);
   const size_t smem = smem_bytes<TY, S>();
   auto kern = step_kernel<TY, S, PERIODIC, FORCE, FLAGS, DIAG>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(d3q27 step)");
-    attr_set = true;
-  }
+  const int rc = set_smem_attr(reinterpret_cast<const void*>(kern), int(smem), "cudaFuncSetAttribute(d3q27 step)");
+  if (rc != HL_OK) return rc;
   kern<<<p.grid, Tile<TY>::THREADS, smem, st>>>(a);
   HL_LAUNCH_CHECK("d3q27 stream_collide launch");
   return HL_OK;

@@ -710,16 +710,7 @@ std::map<const void*, BatchInfo> g_lb;
 
 template <class S> int launch_batch(const void* desc, const BatchInfo& b, int parity, int32_t* work, cudaStream_t st);
 
-int num_sms_local() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
-  return n;
-}
+int num_sms_local() { return device_sms(); }
 
 int box_side_of(float max_bound_radius) { return int(ceilf(2.f * (max_bound_radius + 2.f))) + 2; }
 

@@ -747,12 +747,8 @@ int launch(const hl_world3d* w, double vis, const hl_diag* diag, cudaStream_t st
       return HL_ERR_UNSUPPORTED;
     }
   }
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(d3q27 tma)");
-    attr = true;
-  }
+  rc = set_smem_attr(reinterpret_cast<const void*>(kern), G::SMEM, "cudaFuncSetAttribute(d3q27 tma)");
+  if (rc != HL_OK) return rc;
   const int grid = a.n_items < sms ? a.n_items : sms;
   kern<<<grid, THREADS, G::SMEM, st>>>(a, maps, nullptr, 0, 0);
   HL_LAUNCH_CHECK("d3q27 stream_collide (tma) launch");
@@ -799,12 +795,8 @@ int launch_batch(const BatchDomain* doms, int n_doms, int n_items, double vis, c
   Maps maps;
   std::memset(&maps, 0, sizeof(maps));
   auto kern = step_kernel_tma<S, NSTAGE, false, false, false, false, true>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
-    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(d3q27 tma batch)");
-    attr = true;
-  }
+  const int rc = set_smem_attr(reinterpret_cast<const void*>(kern), G::SMEM, "cudaFuncSetAttribute(d3q27 tma batch)");
+  if (rc != HL_OK) return rc;
   const int sms = num_sms();
   const int grid = n_items < sms ? n_items : sms;
   kern<<<grid, THREADS, G::SMEM, st>>>(a, maps, doms, n_doms, parity);

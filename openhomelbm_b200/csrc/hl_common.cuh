@@ -18,6 +18,11 @@ extern int g_tune_d3_chunks;  // hl_set_tuning("d3q27_chunks")
 extern int g_tune_d3_stages;  // hl_set_tuning("d3q27_stages")
 extern int g_tune_d3_link_blocks;  // hl_set_tuning("d3q27_link_blocks")
 
+// Per-device host state (a process may drive several GPUs): the current device's SM count,
+// and the dynamic shared-memory opt-in of a kernel, set once per (kernel, device, size).
+int device_sms();
+int set_smem_attr(const void* kernel, int bytes, const char* what);
+
 #define HL_CHECK_ARG(cond, ...)       \
   do {                                \
     if (!(cond)) {                    \

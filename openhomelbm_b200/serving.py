@@ -504,11 +504,9 @@ class ServeEngine:
         # for the batched form. The automatic split of a lone launch is sized to fill every SM
         # with one domain (a 64^3 domain gets chunks of 4 planes, each reading 2 halo planes
         # and refilling the copy pipeline); resident domains on their own streams fill the GPU
-        # together, so whole columns spend less on halos and fills. Measured on a B200, 48
-        # requests over 32 slots: control-step p50 24.1 ms automatic, 21.9 ms with 1, and
-        # 1363-1375 env-steps/s against 911-1250. The batched launch is the opposite case: its
-        # items of 64-192 planes would end on the longest ones, so it keeps its own ~32-plane
-        # chunks (p50 27.0 ms; 29.4 ms with whole columns).
+        # together, so whole columns spend less on halos and fills. The batched launch is the
+        # opposite case: its items of 64-192 planes would end on the longest ones, so it keeps
+        # its own ~32-plane chunks.
         if x_chunks is None:
             x_chunks = 0 if self.batched else 1
         self.x_chunks = int(x_chunks)
@@ -516,9 +514,8 @@ class ServeEngine:
             raise ValueError(f"x_chunks must be >= 0, got {x_chunks}")
         # blocks of each domain's cut-link kernel (the library's "d3q27_link_blocks" while run()
         # lasts; 0 keeps the library's 4 per SM). None: one per SM for per-domain graphs, 0 for
-        # the batched form. With resident domains sharing the GPU, one block per SM left the
-        # other domains' kernels more room: control-step p50 21.65-21.70 ms at 148-296 blocks
-        # against 22.0 ms at the automatic 592 (and 23.0 ms at 37).
+        # the batched form: with resident domains sharing the GPU, fewer blocks per domain leave
+        # the other domains' kernels room.
         if link_blocks is None:
             link_blocks = 0 if self.batched else torch.cuda.get_device_properties(self.device).multi_processor_count
         self.link_blocks = int(link_blocks)

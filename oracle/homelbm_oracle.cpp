@@ -478,15 +478,18 @@ template <class T> void get_cutcell_3d(const Solids3<T>& s, const V3<T>& o, cons
 
 // stream_and_collide_3d, envs/lbm3d/lbm_func_3d.py:364-604, for x-planes [x0, x1).
 template <class T>
-void stream_collide_3d_planes(const Params3<T>& p, const Solids3<T>& s, const T* cur, T* post, const int* flag,
-                              const T* force, int x0, int x1, T* loads) {
+void stream_collide_3d_rows(const Params3<T>& p, const Solids3<T>& s, const T* cur, T* post, const int* flag,
+                            const T* force, int64_t r0, int64_t r1, T* loads) {
   const int nx = p.nx, ny = p.ny, nz = p.nz;
   const size_t N = size_t(nx) * ny * nz;
   const T cs2 = cs2_3d<T>();
   const T* M[10];
   for (int k = 0; k < 10; ++k) M[k] = cur + k * N;
-  for (int x = x0; x < x1; ++x)
-    for (int y = 0; y < ny; ++y)
+  // rows r = x * ny + y in [r0, r1): threads split (x, y) rows, so a thin slab still
+  // gives every thread work
+  for (int64_t r = r0; r < r1; ++r) {
+    const int x = int(r / ny), y = int(r % ny);
+    {
       for (int z = 0; z < nz; ++z) {
         const size_t c = (size_t(x) * ny + y) * nz + z;
         const int fl = flag ? flag[c] : ML_FLUID;
@@ -617,6 +620,8 @@ void stream_collide_3d_planes(const Params3<T>& p, const Solids3<T>& s, const T*
         post[8 * N + c] = pixz * invRho;
         post[9 * N + c] = piyz * invRho;
       }
+    }
+  }
 }
 
 // f_eq_home_3d, envs/lbm3d/lbm_func_3d.py:651-686 (no clamp, unlike 2D)
@@ -694,12 +699,13 @@ void step_3d(const Params3<T>& p, Solids3<T>& s, const T* cur, T* post, const in
   for (int i = 0; i < 6 * s.n_objects; ++i) s.loads[i] = T(0.0);
   const int nt = num_threads(nthreads);
   if (nt <= 1) {
-    stream_collide_3d_planes(p, s, cur, post, flag, force, 0, p.nx, s.loads);
+    stream_collide_3d_rows(p, s, cur, post, flag, force, 0, int64_t(p.nx) * p.ny, s.loads);
   } else {
     std::vector<T> part(size_t(nt) * 6 * s.n_objects + 1, T(0.0));
+    const int64_t rows = int64_t(p.nx) * p.ny;
     parallel_for_threads(nt, [&](int t, int n) {
-      const int x0 = int(int64_t(p.nx) * t / n), x1 = int(int64_t(p.nx) * (t + 1) / n);
-      stream_collide_3d_planes(p, s, cur, post, flag, force, x0, x1, part.data() + size_t(t) * 6 * s.n_objects);
+      const int64_t r0 = rows * t / n, r1 = rows * (t + 1) / n;
+      stream_collide_3d_rows(p, s, cur, post, flag, force, r0, r1, part.data() + size_t(t) * 6 * s.n_objects);
     });
     for (int t = 0; t < nt; ++t)
       for (int i = 0; i < 6 * s.n_objects; ++i) s.loads[i] += part[size_t(t) * 6 * s.n_objects + i];

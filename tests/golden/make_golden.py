@@ -19,7 +19,9 @@ launch them:
 
 Usage (needs the reference source tree; the fixtures it writes are committed):
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference source tree>
+
+(or the HOMELBM_REFERENCE environment variable instead of --reference)
 """
 from __future__ import annotations
 
@@ -405,9 +407,12 @@ def case_init(R, name):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("HOMELBM_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("HOMELBM_REFERENCE"),
+                    help="the reference's source tree (default: $HOMELBM_REFERENCE)")
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("--reference (or HOMELBM_REFERENCE) is required")
     R = import_reference(args.reference)
     circle = np.asarray(R.solid.generate_unit_circle_points(24), np.float32)
     square = np.array([[-1, -1], [1, -1], [1, 1], [-1, 1]], np.float32)

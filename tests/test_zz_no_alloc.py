@@ -151,3 +151,27 @@ def test_noalloc_optional_outputs_and_rejections():
     rc = lib.hl_d3q27_stream_collide_noalloc(ctypes.byref(wh), 0.01, None, None, st)
     assert rc == _lib.HL_ERR_ARG
     assert b"float32 or float64" in lib.hl_last_error()
+
+
+def test_noalloc_back_to_back_on_one_stream():
+    """Two calls queued on one stream with no host synchronisation between them share the one
+    scratch array safely (stream order serialises them); each call's mass and health match the
+    definitions on the field that call wrote."""
+    shape = (24, 16, 32)
+    lib, code, a, b, flag, force = _setup(shape, "float32", True, False)
+    c = torch.empty_like(a)
+    st = _lib.stream_ptr()
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    bad = torch.full((2,), -1, dtype=torch.int32, device="cuda")
+    w1 = _world(shape, code, a, b, True)
+    w2 = _world(shape, code, b, c, True)
+    _lib.check(lib.hl_d3q27_stream_collide_noalloc(ctypes.byref(w1), 0.01, out[0:].data_ptr(), bad[0:].data_ptr(),
+                                                   st), "noalloc 1")
+    _lib.check(lib.hl_d3q27_stream_collide_noalloc(ctypes.byref(w2), 0.01, out[1:].data_ptr(), bad[1:].data_ptr(),
+                                                   st), "noalloc 2")
+    torch.cuda.synchronize()
+    for k, field in enumerate((b, c)):
+        mass, health = _expected_diag(field, None)
+        assert _close(out[k].item(), mass), (k, out[k].item(), mass)
+        assert bad[k].item() == health == 0, (k, bad[k].item(), health)
+    assert out[0].item() != 0.0 and out[1].item() != 0.0
