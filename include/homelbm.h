@@ -196,6 +196,48 @@ HL_API int hl_d3q27_init_tgv(int nx, int ny, int nz, hl_storage storage, void* m
 /* Replaces InitBoundary3D (envs/lbm3d/lbm_func_3d.py:13-19). */
 HL_API int hl_d3q27_init_boundary(int nx, int ny, int nz, int32_t* flag, hl_stream stream);
 
+/* ------------------------------------------------------------------ masked world resets
+ * The reference's flows_wp (a device array of HomeFlow / HomeFlow3D structs,
+ * envs/lbm3d/lbm_solver_3d.py:68, envs/lbm/lbm_solver.py:80) is here a device array of the
+ * descriptors below, one per world; reset kernels read it and a device int32 mask with one entry
+ * per world (non-zero: reset that world), as the reference's kernels do. Parts (what):
+ *   HL_RESET_FLOW            ResetSingleWorldFlow(3D) (envs/lbm/lbm_func.py:66-114,
+ *                            envs/lbm3d/lbm_func_3d.py:86-150): rho = 1, u = 0, S = 0 in both
+ *                            buffers (the reference's rest state, its cs2_local quirk giving
+ *                            S = +0), body force zeroed
+ *   HL_RESET_SOLID_TRANSFORM ResetSingleWorldSolidTransform3D (lbm_func_3d.py:153-175): mesh
+ *                            transforms and last transforms = identity, initialized = 0; in 2D
+ *                            ResetSingleWorldSolidTransform (lbm_func.py:117-140): the first
+ *                            solid_line_num[s] points of both transformed outlines = (0, 0)
+ *   HL_RESET_FORCES          ResetSingleWorldForces(3D) (lbm_func.py:143-160,
+ *                            lbm_func_3d.py:178-196): per-solid force and torque = 0
+ *   HL_RESET_INITIALIZED     3D only: initialized = 0 alone (LBM_Solver3D.reset_world(s),
+ *                            envs/lbm3d/lbm_solver_3d.py:348-385)
+ * One launch does every requested part of every masked world; max_cells is at least the largest
+ * cell count of any world (2D: and its n_objects * max_segments); n_objects <= 256. Pointers
+ * that are NULL are skipped. Stream-ordered, allocation-free, capturable. */
+#define HL_RESET_FLOW 1
+#define HL_RESET_SOLID_TRANSFORM 2
+#define HL_RESET_FORCES 4
+#define HL_RESET_INITIALIZED 8
+
+typedef struct {
+  int nx, ny, nz;
+  hl_storage storage;
+  void* m0;                  /* moment buffer 0 [10][nx][ny][nz] */
+  void* m1;                  /* moment buffer 1 */
+  float* force;              /* [3][nx][ny][nz] forcex, forcey, forcez, or NULL */
+  int n_objects;
+  float* transforms;         /* [n][7] mesh_transforms (p, q x y z w) */
+  float* transforms_last;    /* [n][7] mesh_transforms_last */
+  int32_t* initialized;      /* [n] mesh_transforms_initialized */
+  float* solid_force;        /* [n][3] */
+  float* solid_torque;       /* [n][3] */
+} hl_flow3d;
+
+HL_API int hl_d3q27_reset_worlds(const hl_flow3d* flows, int nworld, hl_dtype dtype, const int32_t* reset_mask,
+                                 int what, long long max_cells, hl_stream stream);
+
 /* Immersed triangle-mesh solids of one 3D world (HomeFlow3D's per-solid fields,
  * envs/lbm3d/lbm_core_3d.py:91-119). Solid k's mesh is the triangles
  * tris[tri_offset[k] .. tri_offset[k+1]) in its body frame, vertices already scaled by
@@ -411,6 +453,29 @@ HL_API int hl_d2q9_init_uniform(int nx, int ny, hl_storage storage, void* m_a, v
                          float ux, float uy, hl_stream stream);
 /* Replaces InitBoundary (envs/lbm/lbm_func.py:17-23). */
 HL_API int hl_d2q9_init_boundary(int nx, int ny, int32_t* flag, hl_stream stream);
+
+/* One world of the 2D flows_wp for hl_d2q9_reset_worlds (see hl_d3q27_reset_worlds). */
+typedef struct {
+  int nx, ny;
+  hl_storage storage;
+  void* m0;                  /* moment buffer 0 [6][nx][ny] */
+  void* m1;                  /* moment buffer 1 */
+  float* forcex;             /* [nx][ny] or NULL */
+  float* forcey;             /* [nx][ny] or NULL */
+  int n_objects, max_segments;
+  const int32_t* line_num;   /* [n] solid_line_num */
+  float* line_tf;            /* [n][max_segments][2] solid_line_transformed */
+  float* line_tf_last;       /* [n][max_segments][2] solid_line_transformed_last */
+  float* solid_forcex;       /* [n] */
+  float* solid_forcey;       /* [n] */
+  float* torque;             /* [n] */
+} hl_flow2d;
+
+/* ResetSingleWorldFlow, ResetSingleWorldSolidTransform and ResetSingleWorldForces
+ * (envs/lbm/lbm_func.py:66-160) over the worlds whose reset_mask entry is non-zero; parts as for
+ * hl_d3q27_reset_worlds (HL_RESET_INITIALIZED is 3D only). */
+HL_API int hl_d2q9_reset_worlds(const hl_flow2d* flows, int nworld, hl_dtype dtype, const int32_t* reset_mask,
+                                int what, long long max_cells, hl_stream stream);
 
 /* Field diagnostics: headless images of a world's current moments (cur), the arithmetic of the
  * reference's display kernels, into a caller-owned binary32 device buffer (no GL texture).

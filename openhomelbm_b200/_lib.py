@@ -73,6 +73,22 @@ class hl_solids2d(Structure):
                 ("band_box", c_void_p)]
 
 
+class hl_flow3d(Structure):
+    _fields_ = [("nx", c_int), ("ny", c_int), ("nz", c_int), ("storage", hl_storage), ("m0", c_void_p),
+                ("m1", c_void_p), ("force", c_void_p), ("n_objects", c_int), ("transforms", c_void_p),
+                ("transforms_last", c_void_p), ("initialized", c_void_p), ("solid_force", c_void_p),
+                ("solid_torque", c_void_p)]
+
+
+class hl_flow2d(Structure):
+    _fields_ = [("nx", c_int), ("ny", c_int), ("storage", hl_storage), ("m0", c_void_p), ("m1", c_void_p),
+                ("forcex", c_void_p), ("forcey", c_void_p), ("n_objects", c_int), ("max_segments", c_int),
+                ("line_num", c_void_p), ("line_tf", c_void_p), ("line_tf_last", c_void_p),
+                ("solid_forcex", c_void_p), ("solid_forcey", c_void_p), ("torque", c_void_p)]
+
+
+HL_RESET_FLOW, HL_RESET_SOLID_TRANSFORM, HL_RESET_FORCES, HL_RESET_INITIALIZED = 1, 2, 4, 8
+
 _lib = None
 
 _SIGS = {
@@ -130,6 +146,8 @@ _SIGS = {
     "hl_d2q9_init_uniform": ([c_int, c_int, hl_storage, c_void_p, c_void_p, c_void_p, c_void_p, c_float,
                               c_float, c_void_p], c_int),
     "hl_d2q9_init_boundary": ([c_int, c_int, c_void_p, c_void_p], c_int),
+    "hl_d3q27_reset_worlds": ([c_void_p, c_int, c_int, c_void_p, c_int, c_longlong, c_void_p], c_int),
+    "hl_d2q9_reset_worlds": ([c_void_p, c_int, c_int, c_void_p, c_int, c_longlong, c_void_p], c_int),
 }
 
 

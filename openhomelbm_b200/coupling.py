@@ -52,6 +52,14 @@ def extract_body_states(xipos, xquat, body_ids, positions_out, quaternions_out) 
                                                 _lib.ptr(po), _lib.ptr(qo), _lib.stream_ptr()), "extract_body_states")
 
 
+def _solver(x):
+    """The solver behind ``x``: a solver itself, or its ``flows_wp`` (the reference passes
+    ``lbm_solver.flows_wp`` as these kernels' first input)."""
+    from ._array import FlowArray
+
+    return x.solver if isinstance(x, FlowArray) else x
+
+
 def _mapping(solver, solid_ids, mujoco_origins, lbm_origins, scales, dim):
     ids = _ids(solid_ids if solid_ids is not None else solver.solid_ids_wp, solver.solid_num, "solid_ids")
     nsel = ids.numel()
@@ -71,7 +79,8 @@ def convert_and_update_solid_batch_3d(solver, solid_ids, mujoco_positions, mujoc
     """convert_and_update_solid_batch_3d on an LBM_Solver3D: lattice positions, quaternions and
     mesh transforms of the selected solids in every world (the current transform moves to
     mesh_transforms_last, which is also set on the first call). Mappings default to the
-    solver's finalize_mappings arrays."""
+    solver's finalize_mappings arrays. ``solver`` may be the solver's ``flows_wp``."""
+    solver = _solver(solver)
     ids, nsel, mo, lo, sc = _mapping(solver, solid_ids, mujoco_origins, lbm_origins, scales, 3)
     W = solver.nworld
     mp = _dev(mujoco_positions, torch.float32, (W, nsel, 3), "mujoco_positions")
@@ -86,7 +95,8 @@ def convert_and_update_solid_batch_3d(solver, solid_ids, mujoco_positions, mujoc
 def convert_and_update_solid_batch_2d(solver, solid_ids, mujoco_positions, mujoco_quaternions, mujoco_origins=None,
                                       lbm_origins=None, scales=None) -> None:
     """convert_and_update_solid_batch_2d on an LBM_Solver: planar positions and yaw angles of the
-    selected solids in every world."""
+    selected solids in every world. ``solver`` may be the solver's ``flows_wp``."""
+    solver = _solver(solver)
     ids, nsel, mo, lo, sc = _mapping(solver, solid_ids, mujoco_origins, lbm_origins, scales, 2)
     W = solver.nworld
     mp = _dev(mujoco_positions, torch.float32, (W, nsel, 3), "mujoco_positions")
@@ -98,6 +108,7 @@ def convert_and_update_solid_batch_2d(solver, solid_ids, mujoco_positions, mujoc
 
 
 def _loads(mode, solver, solid_ids, scales, fconv, tconv, forces_out, torques_out):
+    solver = _solver(solver)
     ids = _ids(solid_ids, solver.solid_num, "solid_ids")
     nsel, W = ids.numel(), solver.nworld
     fo = _dev(forces_out, torch.float32, (W, nsel, 3), "forces_out")

@@ -18,6 +18,7 @@ import numpy as np
 import torch
 
 from .. import _lib
+from .._array import device_array
 
 CX = (0, 1, -1, 0, 0, 1, -1, -1, 1)
 CY = (0, 0, 0, 1, -1, 1, 1, -1, -1)
@@ -75,6 +76,11 @@ class HomeFlow:
         self.loads64 = torch.zeros((n, 3), dtype=torch.float64, device=dev)
         self.band_box = torch.zeros(4, dtype=torch.int32, device=dev)
         self.version = 0
+        # the per-world fields callers read back with numpy(), as from Warp arrays
+        for name in ("flag", "solid_forcex", "solid_forcey", "torque", "mass", "MoI", "solid_position", "solid_angle",
+                     "solid_scale", "solid_mass_center", "solid_max_radius", "solid_line_num", "solid_line",
+                     "solid_line_transformed", "solid_line_transformed_last"):
+            setattr(self, name, device_array(getattr(self, name)))
 
     # ------------------------------------------------------------------ solids
     def configure_solid(self, solid_id: int, lines: Any, position: Any, angle: float = 0.0, scale: float = 0.3,
@@ -99,7 +105,7 @@ class HomeFlow:
                 t = torch.zeros((self.n_objects, nseg, 2), dtype=torch.float32, device=self.device)
                 if name == "solid_line":
                     t[:, :old] = getattr(self, name)
-                setattr(self, name, t)
+                setattr(self, name, device_array(t))
         mc = (0.0, 0.0) if mass_center is None else (float(mass_center[0]), float(mass_center[1]))
         # conservative squared radius in normalised units (lbm_core.py:248-256)
         max_dist = 0.0
@@ -150,20 +156,20 @@ class HomeFlow:
         return out
 
     def _plane(self, k: int, post: bool) -> torch.Tensor:
-        return (self.decoded(post) if self.encoded else (self.post if post else self.cur))[k]
+        return device_array((self.decoded(post) if self.encoded else (self.post if post else self.cur))[k])
 
     rho = property(lambda s: s._plane(0, False))
     rho_post = property(lambda s: s._plane(0, True))
-    u = property(lambda s: (s.decoded(False) if s.encoded else s.cur)[1:3].permute(1, 2, 0))
-    u_post = property(lambda s: (s.decoded(True) if s.encoded else s.post)[1:3].permute(1, 2, 0))
+    u = property(lambda s: device_array((s.decoded(False) if s.encoded else s.cur)[1:3].permute(1, 2, 0)))
+    u_post = property(lambda s: device_array((s.decoded(True) if s.encoded else s.post)[1:3].permute(1, 2, 0)))
     Sxx = property(lambda s: s._plane(3, False))
     Syy = property(lambda s: s._plane(4, False))
     Sxy = property(lambda s: s._plane(5, False))
     Sxx_post = property(lambda s: s._plane(3, True))
     Syy_post = property(lambda s: s._plane(4, True))
     Sxy_post = property(lambda s: s._plane(5, True))
-    forcex = property(lambda s: s.force[0])
-    forcey = property(lambda s: s.force[1])
+    forcex = property(lambda s: device_array(s.force[0]))
+    forcey = property(lambda s: device_array(s.force[1]))
 
     # ------------------------------------------------------------------ ABI structs
     def world_struct(self) -> _lib.hl_world2d:

@@ -13,6 +13,7 @@ import numpy as np
 import torch
 
 from .. import _lib
+from .._array import FlowArray, device_array, mask_tensor, reset as _reset
 from .lbm_core import HomeFlow
 
 
@@ -43,11 +44,12 @@ class LBM_Solver:
         self.solid_angle_all = torch.zeros((W, n), **f32)
         self.solid_loads_all = torch.zeros((W, 3, n), **f32)  # solid_forcex, solid_forcey, torque
         for w, f in enumerate(self.flows):
-            f.solid_position = self.solid_position_all[w]
-            f.solid_angle = self.solid_angle_all[w]
-            f.solid_forcex = self.solid_loads_all[w, 0]
-            f.solid_forcey = self.solid_loads_all[w, 1]
-            f.torque = self.solid_loads_all[w, 2]
+            # views of the batched rows; numpy() reads them back as wp.array.numpy() does
+            f.solid_position = device_array(self.solid_position_all[w])
+            f.solid_angle = device_array(self.solid_angle_all[w])
+            f.solid_forcex = device_array(self.solid_loads_all[w, 0])
+            f.solid_forcey = device_array(self.solid_loads_all[w, 1])
+            f.torque = device_array(self.solid_loads_all[w, 2])
         self.total_steps = 500000
         self.per_frame_t = 500
         L = _lib.lib()
@@ -68,6 +70,15 @@ class LBM_Solver:
         self.scales_wp = None
         self.solid_ids_wp = None
         self.solid_id_to_index = {}
+        # the reference's flows_wp (lbm_solver.py:80): the worlds as a device array
+        self.flows_wp = FlowArray(self, 2)
+
+    def reset_worlds_mask(self, reset_mask, what: int = _lib.HL_RESET_FLOW | _lib.HL_RESET_SOLID_TRANSFORM |
+                          _lib.HL_RESET_FORCES) -> None:
+        """partial_reset's LBM part (envs/lbm/lbm_fluid_env.py:336-363) in one launch: for the
+        worlds whose reset_mask entry is non-zero, ResetSingleWorldFlow, ResetSingleWorldSolidTransform
+        and ResetSingleWorldForces (``what``: a set of HL_RESET_* parts)."""
+        _reset(self.flows_wp, mask_tensor(reset_mask, self.nworld, self.device), what)
 
     # ------------------------------------------------------------------ descriptors
     def _params_key(self):

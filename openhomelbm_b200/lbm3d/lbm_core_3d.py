@@ -16,6 +16,7 @@ import numpy as np
 import torch
 
 from .. import _lib
+from .._array import device_array
 
 # D3Q27 lattice in the reference's order (lbm_core_3d.py:12-35)
 CX = (0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1)
@@ -92,6 +93,12 @@ class HomeFlow3D:
         # reference Initialize: rho = 1, everything else 0, in both buffers
         for m in self.moments:
             m[0].fill_(1.0 if not self.encoded else 0.0)
+        # the per-world fields callers read back with numpy(), as from Warp arrays
+        for name in ("flag", "mass", "MoI", "mesh_ids", "mesh_transforms", "mesh_transforms_last",
+                     "mesh_transforms_initialized", "mesh_scale_sizes", "linear_v", "angle_v", "solid_force",
+                     "solid_position", "solid_torque", "solid_quaternion", "solid_inertia", "solid_inertia_inv",
+                     "solid_bound_radius"):
+            setattr(self, name, device_array(getattr(self, name)))
 
     # ------------------------------------------------------------------ views
     @property
@@ -127,13 +134,13 @@ class HomeFlow3D:
 
     def _plane(self, k: int, post: bool) -> torch.Tensor:
         if self.encoded:
-            return self.decoded(post)[k]
-        return (self.post if post else self.cur)[k]
+            return device_array(self.decoded(post)[k])
+        return device_array((self.post if post else self.cur)[k])
 
     rho = property(lambda s: s._plane(0, False))
     rho_post = property(lambda s: s._plane(0, True))
-    u = property(lambda s: (s.decoded(False) if s.encoded else s.cur)[1:4].permute(1, 2, 3, 0))
-    u_post = property(lambda s: (s.decoded(True) if s.encoded else s.post)[1:4].permute(1, 2, 3, 0))
+    u = property(lambda s: device_array((s.decoded(False) if s.encoded else s.cur)[1:4].permute(1, 2, 3, 0)))
+    u_post = property(lambda s: device_array((s.decoded(True) if s.encoded else s.post)[1:4].permute(1, 2, 3, 0)))
     Sxx = property(lambda s: s._plane(4, False))
     Syy = property(lambda s: s._plane(5, False))
     Szz = property(lambda s: s._plane(6, False))
@@ -146,9 +153,9 @@ class HomeFlow3D:
     Sxy_post = property(lambda s: s._plane(7, True))
     Sxz_post = property(lambda s: s._plane(8, True))
     Syz_post = property(lambda s: s._plane(9, True))
-    forcex = property(lambda s: None if s.force is None else s.force[0])
-    forcey = property(lambda s: None if s.force is None else s.force[1])
-    forcez = property(lambda s: None if s.force is None else s.force[2])
+    forcex = property(lambda s: None if s.force is None else device_array(s.force[0]))
+    forcey = property(lambda s: None if s.force is None else device_array(s.force[1]))
+    forcez = property(lambda s: None if s.force is None else device_array(s.force[2]))
 
     # ------------------------------------------------------------------ ABI structs
     def world_struct(self, parity: Optional[int] = None) -> _lib.hl_world3d:

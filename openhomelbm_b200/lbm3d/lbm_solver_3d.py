@@ -17,6 +17,7 @@ import numpy as np
 import torch
 
 from .. import _lib
+from .._array import FlowArray, device_array, mask_tensor, reset as _reset
 from .lbm_core_3d import HomeFlow3D
 
 
@@ -124,6 +125,8 @@ class LBM_Solver3D:
         self.scales_wp = None
         self.solid_ids_wp = None
         self.solid_id_to_index = {}
+        # the reference's flows_wp (lbm_solver_3d.py:68): the worlds as a device array
+        self.flows_wp = FlowArray(self, 3)
 
     def _batch_solid_state(self) -> None:
         """Per-solid state of all worlds in batched tensors [nworld][n][...]; each world's
@@ -144,17 +147,18 @@ class LBM_Solver3D:
         self.solid_torque_all = torch.zeros((W, n, 3), **f32)
         self.loads64_all = torch.zeros((W, n, 6), dtype=torch.float64, device=dev)
         for w, f in enumerate(self.flows):
-            f.solid_position = self.solid_position_all[w]
-            f.solid_quaternion = self.solid_quaternion_all[w]
-            f.mesh_transforms = self.mesh_transforms_all[w]
-            f.mesh_transforms_last = self.mesh_transforms_last_all[w]
-            f.mesh_transforms_initialized = self.mesh_transforms_initialized_all[w]
-            f.mesh_scale_sizes = self.mesh_scale_sizes_all[w]
-            f.solid_bound_radius = self.solid_bound_radius_all[w]
-            f.linear_v = self.linear_v_all[w]
-            f.angle_v = self.angle_v_all[w]
-            f.solid_force = self.solid_force_all[w]
-            f.solid_torque = self.solid_torque_all[w]
+            # views of the batched rows; numpy() reads them back as wp.array.numpy() does
+            f.solid_position = device_array(self.solid_position_all[w])
+            f.solid_quaternion = device_array(self.solid_quaternion_all[w])
+            f.mesh_transforms = device_array(self.mesh_transforms_all[w])
+            f.mesh_transforms_last = device_array(self.mesh_transforms_last_all[w])
+            f.mesh_transforms_initialized = device_array(self.mesh_transforms_initialized_all[w])
+            f.mesh_scale_sizes = device_array(self.mesh_scale_sizes_all[w])
+            f.solid_bound_radius = device_array(self.solid_bound_radius_all[w])
+            f.linear_v = device_array(self.linear_v_all[w])
+            f.angle_v = device_array(self.angle_v_all[w])
+            f.solid_force = device_array(self.solid_force_all[w])
+            f.solid_torque = device_array(self.solid_torque_all[w])
             f.loads64 = self.loads64_all[w]
 
     def _solids_struct(self, k: int) -> _lib.hl_solids3d:
@@ -277,17 +281,26 @@ class LBM_Solver3D:
                        "set_uniform_flow_3d")
 
     def reset_world(self, world_idx: int) -> None:
-        """ResetSingleWorldFlow3D for one world (lbm_solver_3d.py:348-365)."""
+        """One world's fluid field and transform history (lbm_solver_3d.py:348-365)."""
         self.reset_worlds([world_idx])
 
     def reset_worlds(self, world_indices: Sequence[int]) -> None:
-        L = _lib.lib()
+        """Selected worlds' fluid fields and transform histories (lbm_solver_3d.py:367-385):
+        ResetSingleWorldFlow3D over the mask of those worlds (rho = 1, u = 0, S = 0 in both buffers,
+        body force zeroed) and mesh_transforms_initialized = 0, so the next pose update starts
+        with zero wall velocity. One launch for all of them."""
+        mask = np.zeros(self.nworld, np.int32)
         for i in world_indices:
-            f = self.flows[int(i)]
-            _lib.check(L.hl_d3q27_init_uniform(f.nx, f.ny, f.nz, _lib.hl_storage(f.storage_code, f.u_scale, f.s_scale),
-                                               _lib.ptr(f.moments[0]), _lib.ptr(f.moments[1]), _lib.ptr(f.force),
-                                               0.0, 0.0, 0.0, _lib.stream_ptr()), "ResetSingleWorldFlow3D")
-            f.mesh_transforms_initialized.zero_()
+            i = int(i)
+            if not 0 <= i < self.nworld:
+                raise ValueError(f"world index {i} out of range [0, {self.nworld})")
+            mask[i] = 1
+        self.reset_worlds_mask(mask, _lib.HL_RESET_FLOW | _lib.HL_RESET_INITIALIZED)
+
+    def reset_worlds_mask(self, reset_mask, what: int = _lib.HL_RESET_FLOW | _lib.HL_RESET_INITIALIZED) -> None:
+        """The masked resets over flows_wp (one entry per world, non-zero: reset) in one launch;
+        ``what`` is a set of HL_RESET_* parts (default: what reset_worlds does)."""
+        _reset(self.flows_wp, mask_tensor(reset_mask, self.nworld, self.device), what)
 
     # ------------------------------------------------------------------ solids
     def create_solid_from_mesh(self, solid_id: int, mesh: Any, lbm_position: Optional[Tuple[float, float, float]] = None,
@@ -365,37 +378,56 @@ class LBM_Solver3D:
         self._solid_version += 1
 
     def _update_mesh_transform(self, flow: HomeFlow3D, solid_id: int) -> None:
-        """New mesh transform from solid_position / solid_quaternion (lbm_solver_3d.py:228-254):
+        """New mesh transform from solid_position / solid_quaternion (lbm_solver_3d.py:244-268):
         the first time both transforms are set (zero wall velocity), afterwards the current one
-        becomes the last."""
-        pos = flow.solid_position[solid_id].detach().cpu().numpy()
-        q = flow.solid_quaternion[solid_id].detach().cpu().numpy()  # w, x, y, z
-        new = torch.tensor([pos[0], pos[1], pos[2], q[1], q[2], q[3], q[0]], dtype=torch.float32, device=self.device)
-        if int(flow.mesh_transforms_initialized[solid_id]) == 0:
-            flow.mesh_transforms[solid_id] = new
-            flow.mesh_transforms_last[solid_id] = new
-            flow.mesh_transforms_initialized[solid_id] = 1
-        else:
-            flow.mesh_transforms_last[solid_id] = flow.mesh_transforms[solid_id].clone()
-            flow.mesh_transforms[solid_id] = new
+        becomes the last. Device-side (hl_couple3d_update_solids with the identity mapping), so
+        no host synchronisation."""
+        self._pose_update(flow.world_index, [solid_id], flow.solid_position[solid_id:solid_id + 1],
+                          flow.solid_quaternion[solid_id:solid_id + 1], identity=True)
+
+    def _pose_update(self, world_idx: int, solid_ids, positions, quaternions, identity: bool) -> None:
+        """One launch of the pose-in kernel for one world: positions (n, 3) and quaternions (n, 4,
+        w x y z) of the solids ``solid_ids``, mapped through each solid's MuJoCo mapping unless
+        ``identity``; updates solid_position / solid_quaternion and the mesh transforms."""
+        n = len(solid_ids)
+        dev = self.device
+        ids = torch.as_tensor(np.asarray(solid_ids, np.int32)).to(dev)
+        pos = torch.as_tensor(positions, dtype=torch.float32).reshape(1, n, 3).to(dev).contiguous()
+        quat = torch.as_tensor(quaternions, dtype=torch.float32).reshape(1, n, 4).to(dev).contiguous()
+        mo = np.zeros((n, 3), np.float32)
+        lo = np.zeros((n, 3), np.float32)
+        sc = np.ones(n, np.float32)
+        if not identity:
+            for i, sid in enumerate(solid_ids):
+                m = self.mujoco_mappings.get(int(sid))
+                if m is not None:
+                    mo[i], lo[i], sc[i] = m["mujoco_origin"], m["lbm_origin"], np.float32(m["scale"])
+        mo_t, lo_t, sc_t = (torch.as_tensor(a).to(dev) for a in (mo, lo, sc))
+        W, S = self.nworld, self.solid_num
+        w = int(world_idx)
+        L = _lib.lib()
+        off3, off4, off7 = w * S * 3, w * S * 4, w * S * 7
+        _lib.check(L.hl_couple3d_update_solids(
+            1, S, n, _lib.ptr(ids), _lib.ptr(pos), _lib.ptr(quat), _lib.ptr(mo_t), _lib.ptr(lo_t), _lib.ptr(sc_t),
+            _lib.ptr(self.solid_position_all.view(-1)[off3:]), _lib.ptr(self.solid_quaternion_all.view(-1)[off4:]),
+            _lib.ptr(self.mesh_transforms_all.view(-1)[off7:]), _lib.ptr(self.mesh_transforms_last_all.view(-1)[off7:]),
+            _lib.ptr(self.mesh_transforms_initialized_all.view(-1)[w * S:]), _lib.stream_ptr()),
+            "update_solids_batch")
 
     def update_solids_batch(self, world_idx: int, solid_ids: Sequence[int], positions: np.ndarray,
                             quaternions: np.ndarray) -> None:
         """Poses of several solids of one world from MuJoCo positions (N, 3) and quaternions
-        (N, 4) in (w, x, y, z) order (lbm_solver_3d.py:256-292)."""
-        flow = self.flows[world_idx]
-        positions = np.asarray(positions, np.float32)
-        quaternions = np.asarray(quaternions, np.float32)
-        for i, sid in enumerate(solid_ids):
-            if sid in self.mujoco_mappings:
-                m = self.mujoco_mappings[sid]
-                lbm_pos = (positions[i] - m["mujoco_origin"]) * np.float32(m["scale"]) + m["lbm_origin"]
-            else:
-                lbm_pos = positions[i]
-            flow.solid_position[sid] = torch.tensor(np.asarray(lbm_pos, np.float32), device=self.device)
-            flow.solid_quaternion[sid] = torch.tensor(quaternions[i], device=self.device)
+        (N, 4) in (w, x, y, z) order (lbm_solver_3d.py:270-306): lattice position
+        (pos - mujoco_origin) * scale + lbm_origin where the solid has a mapping (the position as
+        given otherwise), and the mesh transforms, in one launch without host synchronisation."""
+        positions = np.asarray(positions, np.float32).reshape(-1, 3)
+        quaternions = np.asarray(quaternions, np.float32).reshape(-1, 4)
+        if len(positions) != len(solid_ids) or len(quaternions) != len(solid_ids):
+            raise ValueError("positions and quaternions need one row per solid id")
         for sid in solid_ids:
-            self._update_mesh_transform(flow, sid)
+            if not 0 <= int(sid) < self.solid_num:
+                raise ValueError(f"solid_id {sid} out of range [0, {self.solid_num})")
+        self._pose_update(world_idx, list(solid_ids), positions, quaternions, identity=False)
 
     def get_forces_and_torques(self, world_idx: int, solid_ids: Optional[Sequence[int]] = None
                                ) -> Tuple[np.ndarray, np.ndarray]:

@@ -405,6 +405,95 @@ def case_init(R, name):
     print(f"{name}: ok")
 
 
+def case_reset(R, name, seed):
+    """The masked world resets of partial_reset (envs/lbm3d/lbm_fluid_env_3d.py:558-619,
+    envs/lbm/lbm_fluid_env.py:305-372): ResetSingleWorldFlow(3D), ResetSingleWorldSolidTransform(3D)
+    and ResetSingleWorldForces(3D) over three worlds with random state, mask (1, 0, 1) in 3D and
+    (0, 1, 1) in 2D."""
+    wp = R.wp
+    rng = np.random.default_rng(seed)
+    nworld, nsol = 3, 2
+    shape3 = (5, 4, 6)
+    flows3 = []
+    for _ in range(nworld):
+        f = R.core3.HomeFlow3D()
+        f.Initialize(*shape3, n_objects=nsol)
+        _set_moments3d(f, _random_moments3d(rng, shape3))
+        _set_post3d(f, _random_moments3d(rng, shape3))
+        for n in ("forcex", "forcey", "forcez"):
+            getattr(f, n).np[...] = rng.uniform(-1e-3, 1e-3, shape3)
+        f.mesh_transforms.np[...] = rng.uniform(-2, 2, f.mesh_transforms.np.shape)
+        f.mesh_transforms_last.np[...] = rng.uniform(-2, 2, f.mesh_transforms_last.np.shape)
+        f.mesh_transforms_initialized.np[...] = 1
+        f.solid_force.np[...] = rng.uniform(-1, 1, (nsol, 3))
+        f.solid_torque.np[...] = rng.uniform(-1, 1, (nsol, 3))
+        flows3.append(f)
+
+    def snap3(fl):
+        return dict(cur=np.stack([_moments3d(f) for f in fl]), post=np.stack([_moments3d(f, post=True) for f in fl]),
+                    force=np.stack([np.stack([f.forcex.np, f.forcey.np, f.forcez.np]) for f in fl]),
+                    tf=np.stack([f.mesh_transforms.np for f in fl]).astype(np.float32),
+                    tf_last=np.stack([f.mesh_transforms_last.np for f in fl]).astype(np.float32),
+                    initialized=np.stack([f.mesh_transforms_initialized.np for f in fl]).astype(np.int32),
+                    solid_force=np.stack([f.solid_force.np for f in fl]),
+                    solid_torque=np.stack([f.solid_torque.np for f in fl]))
+
+    before3 = {k + "3_before": v.copy() for k, v in snap3(flows3).items()}
+    fw3 = wp.array(flows3, dtype=R.core3.HomeFlow3D)
+    mask3 = np.array([1, 0, 1], np.int32)
+    m3 = wp.array(mask3, dtype=wp.int32)
+    wp.launch(R.func3.ResetSingleWorldFlow3D, dim=(nworld,) + shape3, inputs=[fw3, m3])
+    wp.launch(R.func3.ResetSingleWorldSolidTransform3D, dim=(nworld, nsol, 1), inputs=[fw3, m3])
+    wp.launch(R.func3.ResetSingleWorldForces3D, dim=nworld, inputs=[fw3, m3])
+    after3 = {k + "3_after": v for k, v in snap3(flows3).items()}
+
+    nx, ny = 7, 5
+    square = np.array([[-1, -1], [1, -1], [1, 1], [-1, 1]], np.float32)
+    circle = np.asarray(R.solid.generate_unit_circle_points(6), np.float32)
+    flows2 = []
+    for _ in range(nworld):
+        f = R.core2.HomeFlow()
+        f.Initialize(nx, ny, n_objects=nsol)
+        f.configure_solid(0, square, (2.5, 2.0), angle=0.1, scale=1.0 / nx)
+        f.configure_solid(1, circle, (4.5, 2.5), angle=0.0, scale=0.8 / nx)
+        m = np.empty((6, nx, ny), np.float32)
+        m[0] = 1.0 + rng.uniform(-0.01, 0.01, (nx, ny))
+        m[1:] = rng.uniform(-0.03, 0.03, (5, nx, ny))
+        _set_moments2d(f, m)
+        f.forcex.np[...] = rng.uniform(-1e-3, 1e-3, (nx, ny))
+        f.forcey.np[...] = rng.uniform(-1e-3, 1e-3, (nx, ny))
+        f.solid_line_transformed.np[...] = rng.uniform(0, 7, f.solid_line_transformed.np.shape)
+        f.solid_line_transformed_last.np[...] = rng.uniform(0, 7, f.solid_line_transformed_last.np.shape)
+        f.solid_forcex.np[...] = rng.uniform(-1, 1, nsol)
+        f.solid_forcey.np[...] = rng.uniform(-1, 1, nsol)
+        f.torque.np[...] = rng.uniform(-1, 1, nsol)
+        flows2.append(f)
+
+    def snap2(fl):
+        return dict(cur=np.stack([_moments2d(f) for f in fl]),
+                    post=np.stack([np.stack([f.rho_post.np, f.u_post.np[..., 0], f.u_post.np[..., 1], f.Sxx_post.np,
+                                             f.Syy_post.np, f.Sxy_post.np]) for f in fl]).astype(np.float32),
+                    force=np.stack([np.stack([f.forcex.np, f.forcey.np]) for f in fl]),
+                    line_tf=np.stack([f.solid_line_transformed.np for f in fl]).astype(np.float32),
+                    line_tf_last=np.stack([f.solid_line_transformed_last.np for f in fl]).astype(np.float32),
+                    loads=np.stack([np.stack([f.solid_forcex.np, f.solid_forcey.np, f.torque.np]) for f in fl]))
+
+    before2 = {k + "2_before": v.copy() for k, v in snap2(flows2).items()}
+    fw2 = wp.array(flows2, dtype=R.core2.HomeFlow)
+    mask2 = np.array([0, 1, 1], np.int32)
+    m2 = wp.array(mask2, dtype=wp.int32)
+    max_seg = flows2[0].max_segments_per_object
+    wp.launch(R.func2.ResetSingleWorldFlow, dim=(nworld, nx, ny), inputs=[fw2, m2])
+    wp.launch(R.func2.ResetSingleWorldSolidTransform, dim=(nworld, nsol, max_seg), inputs=[fw2, m2])
+    wp.launch(R.func2.ResetSingleWorldForces, dim=nworld, inputs=[fw2, m2])
+    after2 = {k + "2_after": v for k, v in snap2(flows2).items()}
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), mask3=mask3, mask2=mask2,
+                        solid_line=np.stack([f.solid_line.np for f in flows2[:1]])[0].astype(np.float32),
+                        solid_line_num=flows2[0].solid_line_num.np.astype(np.int32),
+                        **before3, **after3, **before2, **after2)
+    print(f"{name}: ok")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("HOMELBM_REFERENCE"),
@@ -443,6 +532,7 @@ def main():
                       axis=(0.3, 1.0, 0.2), omega=0.05)),
         "coupling": lambda: case_coupling(R, "coupling", 31),
         "init": lambda: case_init(R, "init"),
+        "reset": lambda: case_reset(R, "reset", 41),
     }
     for k, fn in cases.items():
         if args.only and k not in args.only.split(","):
