@@ -60,7 +60,7 @@ def import_reference(ref):
     stub = types.ModuleType("refenvs.lbm.lbm_fluid_env")
     stub.LBMFluidEnv = object
     sys.modules["refenvs.lbm.lbm_fluid_env"] = stub
-    mods = types.SimpleNamespace(wp=wp)
+    mods = types.SimpleNamespace(wp=wp, root=ref)
     mods.core2 = importlib.import_module("refenvs.lbm.lbm_core")
     mods.func2 = importlib.import_module("refenvs.lbm.lbm_func")
     mods.solid = importlib.import_module("refenvs.lbm.solid_func")
@@ -494,6 +494,149 @@ def case_reset(R, name, seed):
     print(f"{name}: ok")
 
 
+def _tool_kernels(R, path, names, extra_globals):
+    """The @wp.kernel / @wp.func definitions ``names`` (and the module-level ``_LIVE*`` constants)
+    of a reference tool script, executed under the emulator without importing the script (its
+    imports pull in OpenGL, OpenCV and MuJoCo, which the kernels do not use)."""
+    import ast
+
+    src = open(path).read()
+    tree = ast.parse(src)
+    keep = [n for n in tree.body
+            if (isinstance(n, ast.FunctionDef) and n.name in names)
+            or (isinstance(n, ast.Assign) and all(isinstance(t, ast.Name) and t.id.startswith("_LIVE")
+                                                  for t in n.targets))]
+    mod = ast.Module(body=keep, type_ignores=[])
+    ns = dict(extra_globals)
+    ns.update({"wp": R.wp, "np": np, "math": __import__("math")})
+    # dont_inherit: this script's own `from __future__ import annotations` would turn the kernels'
+    # annotations into strings, and the emulator converts scalar arguments by annotation type
+    exec(compile(mod, path, "exec", dont_inherit=True), ns)
+    return ns
+
+
+def case_diagnostics(R, name, seed):
+    """The display kernels on random fields: 2D get_u_img, get_velocity_rgb, get_vorticity_img,
+    get_vorticity_with_solid_img, get_solid_boundary_img (envs/lbm/lbm_func.py:163-319, 804-866);
+    3D slices and projections with mesh silhouettes (envs/lbm3d/lbm_func_3d.py:753-842, 990-1313);
+    the live 3D view's slice stack and colour map (tools/lbm3d_realtime_control.py:68-182); the
+    2D tool's image colour map and force brush (tools/lbm2d_realtime_control.py:144-157, 417-464).
+    The 3D *_with_solid slices are left out: their inside test is Warp's native
+    mesh_query_point_sign_normal, which the emulator does not restate."""
+    wp = R.wp
+    rng = np.random.default_rng(seed)
+    out = {}
+    # ---- 2D
+    nx, ny = 26, 19
+    f2 = R.core2.HomeFlow()
+    f2.Initialize(nx, ny, n_objects=2)
+    square = np.array([[-1, -1], [1, -1], [1, 1], [-1, 1]], np.float32)
+    circle = np.asarray(R.solid.generate_unit_circle_points(12), np.float32)
+    f2.configure_solid(0, square, (7.3, 8.6), angle=0.35, scale=2.2 / nx)
+    f2.configure_solid(1, circle, (17.8, 10.1), angle=0.0, scale=2.9 / nx)
+    fw2 = wp.array([f2], dtype=R.core2.HomeFlow)
+    wp.launch(R.func2.InitBoundary, dim=(1, nx, ny), inputs=[fw2])
+    m = np.zeros((6, nx, ny), np.float32)
+    m[0] = 1.0
+    m[1] = rng.uniform(-0.06, 0.06, (nx, ny))
+    m[2] = rng.uniform(-0.06, 0.06, (nx, ny))
+    _set_moments2d(f2, m)
+    wp.launch(R.func2.precompute_transformed_segments, dim=(1, 2, f2.max_segments_per_object), inputs=[fw2])
+    out["u2"] = m[1:3].copy()
+    out["line_tf2"] = f2.solid_line_transformed.np.copy()
+    out["line_num2"] = f2.solid_line_num.np.astype(np.int32)
+    out["position2"] = f2.solid_position.np.copy()
+    out["scale2"] = f2.solid_scale.np.copy()
+    out["max_radius2"] = f2.solid_max_radius.np.copy()
+    out["grid_length2"] = np.float32(f2.grid_length)
+    wp.launch(R.func2.get_u_img, dim=(nx, ny), inputs=[f2])
+    out["u_img"] = f2.u_img.np.copy()
+    wp.launch(R.func2.get_velocity_rgb, dim=(nx, ny), inputs=[f2, 0.05])
+    out["velocity_rgb"] = f2.u_img_rgb.np.copy()
+    wp.launch(R.func2.get_vorticity_img, dim=(nx, ny), inputs=[f2])
+    out["vorticity2"] = f2.u_img.np.copy()
+    wp.launch(R.func2.get_vorticity_with_solid_img, dim=(nx, ny), inputs=[f2, 1.3])
+    out["vorticity2_solid"] = f2.u_img.np.copy()
+    wp.launch(R.func2.get_solid_boundary_img, dim=(nx, ny), inputs=[f2, 1.3])
+    out["solid_boundary2"] = f2.u_img.np.copy()
+    # ---- 2D tool kernels
+    t2 = _tool_kernels(R, os.path.join(R.root, "tools", "lbm2d_realtime_control.py"),
+                       {"lbm_uimg_to_rgba_kernel", "set_local_force_kernel", "_clamp01"},
+                       {"HomeFlow": R.core2.HomeFlow})
+    for mode, img_key, vmax in ((0, "u_img", 0.06), (1, "vorticity2", 0.02), (2, "solid_boundary2", 1.0)):
+        f2.u_img.np[...] = out[img_key]
+        rgba = wp.zeros((ny, nx, 4), dtype=wp.uint8)
+        wp.launch(t2["lbm_uimg_to_rgba_kernel"], dim=(nx, ny), inputs=[f2, rgba, mode, vmax])
+        out[f"uimg_rgba_{mode}"] = rgba.np.copy()
+    out["local_force_args"] = np.array([9.5, 7.25, 5.0, 3.5, 2e-4, -1e-4], np.float32)
+    wp.launch(t2["set_local_force_kernel"], dim=(1, nx, ny), inputs=[fw2, *[float(v) for v in out["local_force_args"]]])
+    out["local_force"] = np.stack([f2.forcex.np, f2.forcey.np]).copy()
+    # ---- 3D
+    shape = (14, 12, 10)
+    f3 = R.core3.HomeFlow3D()
+    f3.Initialize(*shape, n_objects=1)
+    fw3 = wp.array([f3], dtype=R.core3.HomeFlow3D)
+    wp.launch(R.func3.InitBoundary3D, dim=(1,) + shape, inputs=[fw3])
+    m3 = _random_moments3d(rng, shape)
+    m3[1:4] *= np.float32(1.5)
+    _set_moments3d(f3, m3)
+    verts, faces = _octahedron(3.1)
+    mesh = wp.Mesh(points=wp.array(verts, dtype=wp.vec3), indices=wp.array(faces.ravel(), dtype=wp.int32))
+    f3.mesh_ids.np[0] = mesh.id
+    f3.mesh_scale_sizes.np[0] = (1.0, 1.2, 0.9)
+    q = _quat_wxyz((0.2, 1.0, 0.4), 0.7)
+    f3.mesh_transforms.np[0] = (6.3, 5.6, 4.7, q[1], q[2], q[3], q[0])
+    out["u3"] = m3[1:4].copy()
+    out["flag3"] = f3.flag.np.copy()
+    out["grid_length3"] = np.float32(f3.grid_length)
+    out["mesh_vertices"], out["mesh_faces"] = verts, faces
+    out["mesh_transform"] = f3.mesh_transforms.np[0].astype(np.float32).copy()
+    out["mesh_scale"] = f3.mesh_scale_sizes.np[0].astype(np.float32).copy()
+    nx3, ny3, nz3 = shape
+    for kern, dim, arg, field, key in (
+            (R.func3.get_u_img_xy_3d, (nx3, ny3), 6, "u_img_xy", "u_xy_6"),
+            (R.func3.get_u_img_yz_3d, (ny3, nz3), 5, "u_img_xz", "u_yz_5"),
+            (R.func3.get_vorticity_xy_3d, (nx3, ny3), 3, "u_img_xy", "vort_xy_3"),
+            (R.func3.get_vorticity_yz_3d, (ny3, nz3), 9, "u_img_xz", "vort_yz_9")):
+        wp.launch(kern, dim=dim, inputs=[f3, arg])
+        out[key] = getattr(f3, field).np.copy()
+    for kname, dim, field in (("get_u_projection_topdown_3d", (nx3, ny3), "u_img_xy"),
+                              ("get_u_projection_max_topdown_3d", (nx3, ny3), "u_img_xy"),
+                              ("get_vorticity_projection_topdown_3d", (nx3, ny3), "u_img_xy"),
+                              ("get_u_projection_side_3d", (ny3, nz3), "u_img_xz"),
+                              ("get_u_projection_front_3d", (nx3, nz3), "u_img_xz_front"),
+                              ("get_vorticity_projection_side_3d", (ny3, nz3), "u_img_xz"),
+                              ("get_vorticity_projection_front_3d", (nx3, nz3), "u_img_xz_front")):
+        wp.launch(getattr(R.func3, kname), dim=dim, inputs=[f3])
+        out[kname] = getattr(f3, field).np.copy()
+    # ---- live slice stack
+    t3 = _tool_kernels(R, os.path.join(R.root, "tools", "lbm3d_realtime_control.py"),
+                       {"_extract_live_vorticity_slices", "_live_clamp01", "_live_vorticity_to_rgba"},
+                       {"HomeFlow3D": R.core3.HomeFlow3D})
+    out["live_bins"] = np.int32(t3["_LIVE_HISTOGRAM_BINS"])
+    live = []
+    for slice_axis, color_axis, stride, margin, positions in ((2, 2, 1, 1, (0, 4, 9)), (0, 1, 2, 0, (3, 13)),
+                                                              (1, 0, 3, 2, (6,))):
+        w_ = {0: ny3, 1: nx3, 2: nx3}[slice_axis]
+        h_ = {0: nz3, 1: nz3, 2: ny3}[slice_axis]
+        pw, ph = (w_ + stride - 1) // stride, (h_ + stride - 1) // stride
+        pos = wp.array(np.array(positions, np.int32), dtype=wp.int32)
+        vals = wp.zeros(len(positions) * ph * pw, dtype=wp.float32)
+        hist = wp.zeros(int(t3["_LIVE_HISTOGRAM_BINS"]), dtype=wp.int32)
+        wp.launch(t3["_extract_live_vorticity_slices"], dim=(pw, ph, len(positions)),
+                  inputs=[f3, pos, vals, hist, pw, ph, stride, slice_axis, color_axis, margin, 1])
+        rgba = wp.zeros(vals.np.size * 4, dtype=wp.uint8)
+        wp.launch(t3["_live_vorticity_to_rgba"], dim=vals.np.size, inputs=[vals, rgba, 0.05, 0.8])
+        live.append(dict(args=np.array([slice_axis, color_axis, stride, margin, pw, ph], np.int32),
+                         positions=np.array(positions, np.int32), values=vals.np.copy(), hist=hist.np.copy(),
+                         rgba=rgba.np.copy()))
+    for k, d in enumerate(live):
+        for kk, v in d.items():
+            out[f"live{k}_{kk}"] = v
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(f"{name}: ok")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("HOMELBM_REFERENCE"),
@@ -533,6 +676,7 @@ def main():
         "coupling": lambda: case_coupling(R, "coupling", 31),
         "init": lambda: case_init(R, "init"),
         "reset": lambda: case_reset(R, "reset", 41),
+        "diagnostics": lambda: case_diagnostics(R, "diagnostics", 43),
     }
     for k, fn in cases.items():
         if args.only and k not in args.only.split(","):

@@ -450,6 +450,10 @@ def abs(x):  # noqa: A001
     return -x if x < 0 else x
 
 
+def log(x):
+    return np.float32(np.log(np.float32(x)))
+
+
 def atomic_add(arr, idx, value):
     k = arr._key(idx)
     if arr.kind == "vec":

@@ -106,3 +106,81 @@ def test_2d_realtime_oracle_maps():
     np.testing.assert_array_equal(od.uimg_rgba(np.array([[0.0, 0.25]], np.float32), 2, 1.0)[:, 0, 0], [255, 191])
     fx, fy = od.local_force(5, 5, 2, 2, 2, 2, 1.0, -2.0)
     assert fx[2, 2] == 1.0 and fy[2, 2] == -2.0 and fx[0, 0] == 0 and fx[2, 3] == np.float32(0.75)
+
+
+# --------------------------------------------------------------------------- pinned to the reference
+def _golden():
+    from conftest import load_golden
+
+    return load_golden("diagnostics")
+
+
+def test_2d_display_kernels_match_reference_fixture():
+    """oracle/diagnostics.py against the reference's own 2D display kernels (get_u_img,
+    get_velocity_rgb, get_vorticity_img, get_vorticity_with_solid_img, get_solid_boundary_img,
+    envs/lbm/lbm_func.py:163-319, 804-866) and the 2D tool's kernels (lbm_uimg_to_rgba_kernel,
+    set_local_force_kernel, tools/lbm2d_realtime_control.py:144-157, 417-464), run under the
+    Warp emulator by tests/golden/make_golden.py: bit for bit."""
+    g = _golden()
+    u = g["u2"]
+    nx, ny = u.shape[1:]
+    np.testing.assert_array_equal(od.u_img(u), g["u_img"])
+    np.testing.assert_array_equal(od.velocity_rgb(u, 0.05), g["velocity_rgb"])
+    vort = od.vorticity_2d(u, g["grid_length2"])
+    np.testing.assert_array_equal(vort, g["vorticity2"])
+    mask = od.solid_mask_2d(nx, ny, g["line_tf2"], g["line_num2"], g["position2"], g["scale2"], g["max_radius2"], 1.3)
+    assert 20 < mask.sum() < mask.size // 2
+    np.testing.assert_array_equal(np.where(mask, od.SOLID_MARK, vort), g["vorticity2_solid"])
+    np.testing.assert_array_equal(mask.astype(np.float32), g["solid_boundary2"])
+    for mode, key, vmax in ((0, "u_img", 0.06), (1, "vorticity2", 0.02), (2, "solid_boundary2", 1.0)):
+        np.testing.assert_array_equal(od.uimg_rgba(g[key], mode, vmax), g[f"uimg_rgba_{mode}"], err_msg=str(mode))
+    fx, fy = od.local_force(nx, ny, *g["local_force_args"])
+    np.testing.assert_array_equal(np.stack([fx, fy]), g["local_force"])
+
+
+def test_3d_display_kernels_match_reference_fixture():
+    """The 3D slices and projections, silhouettes of a scaled, rotated mesh included
+    (envs/lbm3d/lbm_func_3d.py:320-362, 753-842, 990-1313), against the reference's kernels
+    under the emulator, bit for bit. The ray queries of the silhouettes are Warp's native
+    mesh_query_ray in the reference and a Moller-Trumbore restatement in the emulator and here."""
+    g = _golden()
+    u = g["u3"]
+    h = g["grid_length3"]
+    flag = g["flag3"]
+    mag = np.sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2])
+    np.testing.assert_array_equal(od.plane(mag, 2, 6), g["u_xy_6"])
+    np.testing.assert_array_equal(od.plane(mag, 0, 5), g["u_yz_5"])
+    np.testing.assert_array_equal(od.plane(od.vorticity_3d(u, 2, h), 2, 3), g["vort_xy_3"])
+    np.testing.assert_array_equal(od.plane(od.vorticity_3d(u, 0, h), 0, 9), g["vort_yz_9"])
+    tris = g["mesh_vertices"][g["mesh_faces"]].astype(np.float32)
+    tri_offset = np.array([0, len(tris)], np.int32)
+    xf, sc = g["mesh_transform"][None], g["mesh_scale"][None]
+    shape = u.shape[1:]
+    sil = {a: od.silhouette(shape, a, tri_offset, tris, xf, sc) for a in (0, 1, 2)}
+    for name, axis, kind in (("get_u_projection_topdown_3d", 2, 1), ("get_u_projection_max_topdown_3d", 2, 0),
+                             ("get_vorticity_projection_topdown_3d", 2, 2), ("get_u_projection_side_3d", 0, 0),
+                             ("get_u_projection_front_3d", 1, 0), ("get_vorticity_projection_side_3d", 0, 2),
+                             ("get_vorticity_projection_front_3d", 1, 2)):
+        assert sil[axis].sum() > 5
+        ref = np.where(sil[axis], od.SOLID_MARK, od.projection(u, axis, kind, h, flag))
+        np.testing.assert_array_equal(ref, g[name], err_msg=name)
+
+
+def test_live_view_kernels_match_reference_fixture():
+    """The live 3D view's slice stack, histogram and colour map
+    (tools/lbm3d_realtime_control.py:68-182) against the reference's kernels under the emulator:
+    values and RGBA bytes bit for bit; histogram counts equal except for values within 1e-4 of a
+    bin edge (the emulator's binary32 logarithm, the oracle's binary64 one)."""
+    g = _golden()
+    u = g["u3"]
+    assert int(g["live_bins"]) == od.LIVE_BINS
+    k = 0
+    while f"live{k}_args" in g:
+        slice_axis, color_axis, stride, margin, pw, ph = (int(v) for v in g[f"live{k}_args"])
+        vals = od.live_slices(u, g[f"live{k}_positions"], pw, ph, stride, slice_axis, color_axis, margin)
+        np.testing.assert_array_equal(vals, g[f"live{k}_values"], err_msg=str(k))
+        hist, near_edge = od.live_histogram(vals)
+        assert np.abs(hist - g[f"live{k}_hist"]).sum() <= 2 * near_edge, k
+        np.testing.assert_array_equal(od.live_rgba(vals, 0.05, 0.8).reshape(-1), g[f"live{k}_rgba"], err_msg=str(k))
+        k += 1
+    assert k == 3
