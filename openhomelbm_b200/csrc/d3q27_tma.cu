@@ -21,12 +21,13 @@
 // plane s0 + 1), so each arithmetic instruction is a packed FADD2 / FMUL2 / FFMA2 serving two
 // cells, and the mailbox entries are 8-byte pairs. A thread rebuilds the 27 populations of
 // its cell pair, keeps the three with c_y = c_z = 0 in registers and writes the other 24 to
-// the mailbox slot of the destination cell (threads 0..99 add the 9 or 3 populations a halo
-// cell sends into the tile). After a block barrier each thread reads its 24 incoming pairs,
+// the mailbox slots of the destination cell, the three c_x of one (c_y, c_z) direction as one
+// 16-byte and one 8-byte entry (threads 0..99 add the 9 or 3 populations a halo cell sends into
+// the tile). After a block barrier each thread reads its 24 incoming pairs,
 // forms the sums of the c_x = -1, 0, +1 groups, and completes the destination planes s0 - 1
 // and s0 from them and from the previous pair's sums. Four stages keep the next pair in
-// flight while the current one is computed. Two block barriers per pair (one per plane); with
-// the reduced storages the second is a split arrive/wait on an mbarrier.
+// flight while the current one is computed. One block barrier per pair (mailbox written); the
+// mailbox's reuse by the next pair is a split arrive/wait on an mbarrier.
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -258,7 +259,11 @@ __global__ void __launch_bounds__(THREADS, 1)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + G::BAR_OFF);
-  P2* mb = reinterpret_cast<P2*>(smem + G::MB_OFF);  // [24 directions][512 destinations]
+  // mailbox by (c_y, c_z) direction (8) and destination (512): the c_x = -1 and 0 populations as
+  // one 16-byte entry, the c_x = +1 one as an 8-byte entry (one STS.128 + one STS.64 per
+  // direction instead of three STS.64, and the same for the loads)
+  float4* mbA = reinterpret_cast<float4*>(smem + G::MB_OFF);                // [8][512]
+  P2* mbB = reinterpret_cast<P2*>(smem + G::MB_OFF + 8 * NDST * 16);       // [8][512]
 
   const int tid = threadIdx.x;
   const int ty = tid / TZ, tz = tid % TZ;
@@ -424,19 +429,16 @@ __global__ void __launch_bounds__(THREADS, 1)
     p_x = xb - 1;
     produce(NSTAGE);
   }
-  // The mailbox is written by every thread before barrier 1 and read after it. With SPLIT,
-  // instead of a second block barrier before the next pair's writes, each warp arrives on
-  // bars[NSTAGE] once it has read its entries, and a thread waits for the phase only before its
-  // next writes: a warp that finished reading goes on to its collision, stores and next rebuild
-  // while the others still read. Measured on a B200 (256^3 periodic Taylor-Green): 2 % faster
-  // with the reduced storages (whose longer encode and stores it overlaps), 1 % slower with
-  // binary32 storage, so the binary32 build keeps the second barrier.
-  constexpr bool SPLIT = S::kEncoded;
+  // The mailbox is written by every thread before barrier 1 and read after it. Instead of a
+  // second block barrier before the next pair's writes, each warp arrives on bars[NSTAGE] once
+  // it has read its entries, and a thread waits for the phase only before its next writes: a
+  // warp that finished reading goes on to its collision, stores and next rebuild while the
+  // others still read.
   const unsigned mb_empty = saddr(&bars[NSTAGE]);
   int mb_phase = 0;
   bool mb_written = false;
   auto wait_mailbox_empty = [&]() {
-    if (SPLIT && mb_written) {
+    if (mb_written) {
       long long spin = 0;
       while (!mbar_try_wait(mb_empty, unsigned(mb_phase))) {
         if (++spin > MAX_SPIN) {
@@ -474,6 +476,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int hgy = y0 - 1 + hsy, hgz = z0 - 1 + hsz;
     const bool h_in = PERIODIC || (hgy >= 0 && hgy < ny && hgz >= 0 && hgz < nz);
     const int dy = y0 + ty, dz = z0 + tz;
+    const int cyz = dy * nz + dz;  // the thread's cell within an x plane
     // group sums of the previous pair that the next destinations still need: all of c_x = +1,
     // the second plane's of c_x = 0
     GroupSums gp_prev;
@@ -509,17 +512,20 @@ __global__ void __launch_bounds__(THREADS, 1)
         P2 f[27];
         rebuild_pair(cf, kc, f);
 #pragma unroll
-        for (int xi = 0; xi < 3; ++xi) {
-          fc[xi] = f[dir_index(xi - 1, 0, 0)];
+        for (int xi = 0; xi < 3; ++xi) fc[xi] = f[dir_index(xi - 1, 0, 0)];
 #pragma unroll
-          for (int yi = 0; yi < 3; ++yi)
+        for (int yi = 0; yi < 3; ++yi)
 #pragma unroll
-            for (int zi = 0; zi < 3; ++zi) {
-              if (yi == 1 && zi == 1) continue;
-              const bool ok = (yi == 0 ? yl_ok : yi == 2 ? yh_ok : true) && (zi == 0 ? zl_ok : zi == 2 ? zh_ok : true);
-              if (ok) mb[mb_dir(xi, yi, zi) * NDST + tid + (yi - 1) * TZ + (zi - 1)] = f[(xi * 3 + yi) * 3 + zi];
+          for (int zi = 0; zi < 3; ++zi) {
+            if (yi == 1 && zi == 1) continue;
+            const bool ok = (yi == 0 ? yl_ok : yi == 2 ? yh_ok : true) && (zi == 0 ? zl_ok : zi == 2 ? zh_ok : true);
+            if (ok) {
+              const int e = mb_dir(0, yi, zi) * NDST + tid + (yi - 1) * TZ + (zi - 1);
+              const P2 a0 = f[(0 * 3 + yi) * 3 + zi], a1 = f[(1 * 3 + yi) * 3 + zi];
+              mbA[e] = make_float4(a0.x(), a0.y(), a1.x(), a1.y());
+              mbB[e] = f[(2 * 3 + yi) * 3 + zi];
             }
-        }
+          }
       }
       if (has_halo) {
         P2 raw[10];
@@ -530,28 +536,38 @@ __global__ void __launch_bounds__(THREADS, 1)
         rebuild_face(cf, kc, h_row, P2(float(hs), float(hs)), f);
 #pragma unroll
         for (int i = 0; i < 3; ++i)
-#pragma unroll
-          for (int xi = 0; xi < 3; ++xi)
-            if (h_ok[i]) mb[(xi * 8 + h_dir[i]) * NDST + h_dst[i]] = f[i][xi];
+          if (h_ok[i]) {
+            const int e = h_dir[i] * NDST + h_dst[i];
+            mbA[e] = make_float4(f[i][0].x(), f[i][0].y(), f[i][1].x(), f[i][1].y());
+            mbB[e] = f[i][2];
+          }
       }
       __syncthreads();  // mailbox complete; every thread is done with both stages
       if (tid == 0) produce(has1 ? 2 : 1);
 
       GroupSums g[3];
-#pragma unroll
-      for (int xi = 0; xi < 3; ++xi) {
-        P2 p[3][3];
+      {
+        P2 p[3][3][3];  // [xi][yi][zi]
 #pragma unroll
         for (int yi = 0; yi < 3; ++yi)
 #pragma unroll
-          for (int zi = 0; zi < 3; ++zi)
-            p[yi][zi] = (yi == 1 && zi == 1) ? fc[xi] : mb[mb_dir(xi, yi, zi) * NDST + tid];
-        g[xi] = group_sums(p);
+          for (int zi = 0; zi < 3; ++zi) {
+            if (yi == 1 && zi == 1) {
+#pragma unroll
+              for (int xi = 0; xi < 3; ++xi) p[xi][1][1] = fc[xi];
+              continue;
+            }
+            const int e = mb_dir(0, yi, zi) * NDST + tid;
+            const float4 a = mbA[e];
+            p[0][yi][zi] = P2(a.x, a.y);
+            p[1][yi][zi] = P2(a.z, a.w);
+            p[2][yi][zi] = mbB[e];
+          }
+#pragma unroll
+        for (int xi = 0; xi < 3; ++xi) g[xi] = group_sums(p[xi]);
       }
-      if constexpr (SPLIT) {
-        __syncwarp();
-        if ((tid & 31) == 0) mbar_arrive(mb_empty);  // this warp is done with the mailbox
-      }
+      __syncwarp();
+      if ((tid & 31) == 0) mbar_arrive(mb_empty);  // this warp is done with the mailbox
       // destinations d0 = s0 - 1 and d1 = s0: c_x = -1 populations from (s0, s1), c_x = +1
       // from the previous pair (s0 - 2, s0 - 1), c_x = 0 from (s0 - 1, s0)
       const GroupSums& gm = g[0];
@@ -578,7 +594,9 @@ __global__ void __launch_bounds__(THREADS, 1)
       const int d0 = s0 - 1;
       const bool v0 = d0 >= xb && d0 < xe, v1 = d0 + 1 >= xb && d0 + 1 < xe;
       if (v0 || v1) {
-        const long long c0 = (long long)d0 * plane + (long long)dy * nz + dz, c1 = c0 + plane;
+        const long long c0 = (long long)d0 * plane + cyz, c1 = c0 + plane;
+        T* const q0 = post + c0;  // moment k of the two cells: q0[k * N], q1[k * N]
+        T* const q1 = q0 + plane;
         bool f0 = v0, f1 = v1;
         if (FLAGS) {
           f0 = f0 && a.flag[c0] == ML_FLUID;
@@ -606,20 +624,20 @@ __global__ void __launch_bounds__(THREADS, 1)
             for (int k = 0; k < 10; ++k) d[k] = S::round2(raw[k].x(), raw[k].y(), cs0, cs1, unsigned(k));
             if (f0) {
 #pragma unroll
-              for (int k = 0; k < 10; ++k) post[k * N + c0] = S::hi(d[k]);
+              for (int k = 0; k < 10; ++k) q0[k * N] = S::hi(d[k]);
             }
             if (f1) {
 #pragma unroll
-              for (int k = 0; k < 10; ++k) post[k * N + c1] = S::lo(d[k]);
+              for (int k = 0; k < 10; ++k) q1[k * N] = S::lo(d[k]);
             }
           } else {
             if (f0) {
 #pragma unroll
-              for (int k = 0; k < 10; ++k) post[k * N + c0] = S::from_r_cell(raw[k].x(), cs0, unsigned(k));
+              for (int k = 0; k < 10; ++k) q0[k * N] = S::from_r_cell(raw[k].x(), cs0, unsigned(k));
             }
             if (f1) {
 #pragma unroll
-              for (int k = 0; k < 10; ++k) post[k * N + c1] = S::from_r_cell(raw[k].y(), cs1, unsigned(k));
+              for (int k = 0; k < 10; ++k) q1[k * N] = S::from_r_cell(raw[k].y(), cs1, unsigned(k));
             }
           }
           if (DIAG) {
@@ -635,7 +653,6 @@ __global__ void __launch_bounds__(THREADS, 1)
           }
         }
       }
-      if constexpr (!SPLIT) __syncthreads();  // every thread has read the mailbox: the next pair may overwrite it
     }
   }
   if (timed_out && a.status) atomicExch(a.status, HL_ERR_TIMEOUT);
