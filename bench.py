@@ -48,7 +48,7 @@ def measured_peaks():
 
 # DRAM bytes (read + write) per cell of one stream-collide launch, from one ncu capture of
 # the 256^3 bench workload (profiles/d3q27_stream_collide_tma_256_dram.md).
-DRAM_BYTES_PER_CELL = {"float32": 1320.4e6 / 256 ** 3, "float16": 644.9e6 / 256 ** 3}
+DRAM_BYTES_PER_CELL = {"float32": 1320.1e6 / 256 ** 3, "float16": 643.2e6 / 256 ** 3}
 
 
 def profile_traffic(n, storage):
