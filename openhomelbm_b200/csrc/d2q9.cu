@@ -97,30 +97,42 @@ template <class R> __device__ __forceinline__ R feq_dev_clamped_a(const Mom2<R>&
 
 // Moment-space collision of stream_and_collide (envs/lbm/lbm_func.py:414-467) from deviation
 // populations pop[i] = f_i - w_i: rho = 1 + sum pop, Pi_aa = 1/3 + (deviation sum), and the
-// reference's S_aa = Pi_aa/rho - 1/3 equals X_aa / rho with no cancellation.
+// reference's S_aa = Pi_aa/rho - 1/3 equals X_aa / rho with no cancellation. Written with the
+// explicitly rounded operations, like the population arithmetic: every D2Q9 kernel (gridded,
+// tile, strip and band) then collides a cell to the same number, whatever the compiler would
+// contract in its surroundings. Multiplications by 0.5 are exact.
 template <class R> __device__ __forceinline__ Mom2<R> collide(const R pop[9], R Fx, R Fy, R omega) {
-  const R drho = pop[0] + pop[1] + pop[2] + pop[3] + pop[4] + pop[5] + pop[6] + pop[7] + pop[8];
-  const R rho = R(1) + drho;
+  R drho = add_rn(pop[0], pop[1]);
+#pragma unroll
+  for (int i = 2; i < 9; ++i) drho = add_rn(drho, pop[i]);
+  const R rho = add_rn(R(1), drho);
   const R inv = R(1) / rho;
-  const R ux = (pop[1] - pop[2] + pop[5] - pop[6] - pop[7] + pop[8] + R(0.5) * Fx) * inv;
-  const R uy = (pop[3] - pop[4] + pop[5] + pop[6] - pop[7] - pop[8] + R(0.5) * Fy) * inv;
-  const R pixx0 = pop[1] + pop[2] + pop[5] + pop[6] + pop[7] + pop[8];
-  const R piyy0 = pop[3] + pop[4] + pop[5] + pop[6] + pop[7] + pop[8];
-  const R pixy0 = pop[5] + pop[7] - pop[6] - pop[8];
-  const R Ru2 = rho * ux * ux, Rv2 = rho * uy * uy;
-  const R pxx_part = (pixx0 - piyy0) * R(0.5), pyy_part = (piyy0 - pixx0) * R(0.5);
-  const R o1 = R(1) - omega, oh = (R(1) + omega) * R(0.5), om = o1 * R(0.5);
-  const R pixy = o1 * pixy0 + ux * uy * rho * omega + (R(1) - R(0.5) * omega) * (Fy * ux + Fx * uy);
-  const R xxx = pxx_part * o1 + oh * Ru2 + om * Rv2 + Fx * ux + om * (Fx * ux - Fy * uy);
-  const R xyy = pyy_part * o1 + oh * Rv2 + om * Ru2 + Fy * uy + om * (Fy * uy - Fx * ux);
+  const R half = R(0.5);
+  const R jx = add_rn(add_rn(add_rn(add_rn(add_rn(add_rn(pop[1], -pop[2]), pop[5]), -pop[6]), -pop[7]), pop[8]),
+                      mul_rn(half, Fx));
+  const R jy = add_rn(add_rn(add_rn(add_rn(add_rn(add_rn(pop[3], -pop[4]), pop[5]), pop[6]), -pop[7]), -pop[8]),
+                      mul_rn(half, Fy));
+  const R ux = mul_rn(jx, inv), uy = mul_rn(jy, inv);
+  const R pixx0 = add_rn(add_rn(add_rn(add_rn(add_rn(pop[1], pop[2]), pop[5]), pop[6]), pop[7]), pop[8]);
+  const R piyy0 = add_rn(add_rn(add_rn(add_rn(add_rn(pop[3], pop[4]), pop[5]), pop[6]), pop[7]), pop[8]);
+  const R pixy0 = add_rn(add_rn(add_rn(pop[5], pop[7]), -pop[6]), -pop[8]);
+  const R Ru2 = mul_rn(mul_rn(rho, ux), ux), Rv2 = mul_rn(mul_rn(rho, uy), uy);
+  const R pxx_part = mul_rn(add_rn(pixx0, -piyy0), half), pyy_part = mul_rn(add_rn(piyy0, -pixx0), half);
+  const R o1 = add_rn(R(1), -omega), oh = mul_rn(add_rn(R(1), omega), half), om = mul_rn(o1, half);
+  const R fu = mul_rn(Fx, ux), fv = mul_rn(Fy, uy);
+  const R pixy = fma_rn(o1, pixy0,
+                        add_rn(mul_rn(mul_rn(mul_rn(ux, uy), rho), omega),
+                               mul_rn(add_rn(R(1), -mul_rn(half, omega)), fma_rn(Fy, ux, mul_rn(Fx, uy)))));
+  const R xxx = fma_rn(om, add_rn(fu, -fv), add_rn(fma_rn(om, Rv2, fma_rn(pxx_part, o1, mul_rn(oh, Ru2))), fu));
+  const R xyy = fma_rn(om, add_rn(fv, -fu), add_rn(fma_rn(om, Ru2, fma_rn(pyy_part, o1, mul_rn(oh, Rv2))), fv));
   Mom2<R> m;
   m.rho = rho;
   m.drho = drho;
-  m.ux = ux + Fx * inv * R(0.5);
-  m.uy = uy + Fy * inv * R(0.5);
-  m.sxx = xxx * inv;
-  m.syy = xyy * inv;
-  m.sxy = pixy * inv;
+  m.ux = fma_rn(mul_rn(Fx, inv), half, ux);
+  m.uy = fma_rn(mul_rn(Fy, inv), half, uy);
+  m.sxx = mul_rn(xxx, inv);
+  m.syy = mul_rn(xyy, inv);
+  m.sxy = mul_rn(pixy, inv);
   return m;
 }
 
@@ -387,6 +399,103 @@ __global__ void __launch_bounds__(TILE_THREADS) stream_tiles_kernel(const __grid
       const unsigned cs = unsigned(ci) * 0x9e3779b9u;  // as store2
 #pragma unroll
       for (int k = 0; k < 6; ++k) post[k * N + ci] = S::from_r_cell(raw[k], cs, unsigned(k));
+    }
+  }
+}
+
+// ------------------------------------------------------------- 2c. stream over strips (a warp each)
+// Strip tiles of the work list: TX planes along x by STRIP_Y = 30 rows along y, one warp each.
+// Lane l holds row y0 - 1 + l (lanes 0 and 31 are the strip's halo rows) and the warp marches its
+// source planes x0 - 1 .. x0 + TX. Each lane rebuilds its source cell's nine clamped populations
+// (feq_dev_clamped_a on its decoded moments, -w_i for a source outside a walled world: the same
+// values as stream_kernel), the populations with c_y = +-1 move one lane by a warp shuffle, and
+// those with c_x = 0, +1 wait in registers for the next source planes: once source plane x_s is
+// read, destination plane x_s - 1 has all nine of its populations, and the lanes of rows
+// y0 .. y0 + 29 collide and store it with stream_kernel's collide and store. No shared memory and
+// no block barrier; a strip needs 32/30 of the source work of its cells. Results are identical to
+// stream_kernel.
+constexpr int STRIP_Y = 30;
+
+template <class S, int TX>
+__global__ void __launch_bounds__(256) stream_strips_kernel(const __grid_constant__ Launch L,
+                                                            const int4* __restrict__ tiles, int n_tiles) {
+  using R = typename S::R;
+  using T = typename S::T;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < n_tiles; t += warps) {
+    const int4 tile = tiles[t];
+    const World& wd = world_of(L, tile.x);
+    const int nx = wd.nx, ny = wd.ny;
+    const bool periodic = wd.periodic != 0;
+    const float* __restrict__ fxp = wd.fx;
+    const float* __restrict__ fyp = wd.fy;
+    const Scale sc = wd.sc;
+    const T* __restrict__ cur = static_cast<const T*>(cur_of(L, wd));
+    T* __restrict__ post = static_cast<T*>(post_of(L, wd));
+    const R omega = omega_of<R>(wd.vis_shear);
+    const long long N = (long long)nx * ny;
+    const int x0 = tile.y, y0 = tile.z;
+    const int x1 = x0 + TX < nx ? x0 + TX : nx;  // destination planes x0 .. x1 - 1
+    const int yr = y0 - 1 + lane;                // this lane's row, before wrapping
+    const int y = periodic ? wrap(yr, ny) : yr;
+    const bool y_in = periodic || (yr >= 0 && yr < ny);
+    const bool dest_lane = lane >= 1 && lane <= STRIP_Y && yr < ny;
+    // incoming populations of the last two source planes: c_x = 0 (i = 0, 3, 4) of the previous
+    // plane, c_x = +1 (i = 1, 5, 8) of the previous two
+    R z0 = R(0), z3 = R(0), z4 = R(0), p1 = R(0), p5 = R(0), p8 = R(0), q1 = R(0), q5 = R(0), q8 = R(0);
+    for (int xs = x0 - 1; xs <= x1; ++xs) {
+      const int xw = periodic ? wrap(xs, nx) : xs;
+      const bool in = y_in && (periodic || (xs >= 0 && xs < nx));
+      R f[9];
+      if (in) {
+        const Mom2<R> m = load2<S>(wd, N, (long long)xw * ny + y, cur);
+        const R axxy = third_xxy<R>(m), axyy = third_xyy<R>(m);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) f[i] = feq_dev_clamped_a<R>(m, axxy, axyy, i);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) f[i] = -w2<R>(i);
+      }
+      // what arrives at this lane's row from source plane xs: c_y = +1 from the lane below,
+      // c_y = -1 from the lane above (lanes 0 and 31 receive garbage; they store nothing)
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {
+        if (cy_of(i) == 1) f[i] = __shfl_up_sync(FULL, f[i], 1);
+        else if (cy_of(i) == -1) f[i] = __shfl_down_sync(FULL, f[i], 1);
+      }
+      const int d = xs - 1;  // the destination plane now complete
+      if (dest_lane && d >= x0 && d < x1) {
+        const long long ci = (long long)d * ny + yr;
+        if (is_fluid(wd, d, yr, ci)) {
+          R pop[9];
+          pop[0] = z0;
+          pop[3] = z3;
+          pop[4] = z4;
+          pop[1] = q1;
+          pop[5] = q5;
+          pop[8] = q8;
+          pop[2] = f[2];
+          pop[6] = f[6];
+          pop[7] = f[7];
+          const R Fx = fxp ? R(fxp[ci]) : R(0), Fy = fyp ? R(fyp[ci]) : R(0);
+          R raw[6];
+          encode2<S>(collide<R>(pop, Fx, Fy, omega), sc, raw);
+          const unsigned cs = unsigned(ci) * 0x9e3779b9u;  // as store2
+#pragma unroll
+          for (int k = 0; k < 6; ++k) post[k * N + ci] = S::from_r_cell(raw[k], cs, unsigned(k));
+        }
+      }
+      q1 = p1;
+      q5 = p5;
+      q8 = p8;
+      p1 = f[1];
+      p5 = f[5];
+      p8 = f[8];
+      z0 = f[0];
+      z3 = f[3];
+      z4 = f[4];
     }
   }
 }
@@ -797,7 +906,8 @@ int fill_world(const hl_world2d* w, const hl_step2d* p, const hl_bc2d* bc, const
 }
 
 // The tile shapes of the persistent stream launch (cells along x, along y).
-constexpr int TILE_SHAPES[][2] = {{8, 32}, {16, 32}, {4, 64}, {8, 64}, {16, 64}, {8, 128}};
+// Shapes with 30 rows (d2::STRIP_Y) are strips: a warp per tile (stream_strips_kernel).
+constexpr int TILE_SHAPES[][2] = {{8, 32}, {16, 32}, {4, 64}, {8, 64}, {16, 64}, {8, 128}, {32, 30}, {64, 30}, {128, 30}};
 constexpr int N_TILE_SHAPES = int(sizeof(TILE_SHAPES) / sizeof(TILE_SHAPES[0]));
 
 // A tile work-list for the stream phase (NULL: the gridded stream_kernel).
@@ -819,9 +929,23 @@ template <class S, int TX, int TY> int launch_tiles(const d2::Launch& L, const T
   return HL_OK;
 }
 
+template <class S, int TX> int launch_strips(const d2::Launch& L, const TileWork& tw, cudaStream_t st) {
+  // ctas blocks of 8 warps, a warp per strip, no more blocks than the strips fill
+  const int need = (tw.n_tiles + 7) / 8;
+  const int grid = need < tw.ctas ? need : tw.ctas;
+  d2::stream_strips_kernel<S, TX><<<grid, 256, 0, st>>>(L, tw.tiles, tw.n_tiles);
+  HL_LAUNCH_CHECK("d2q9 stream_and_collide (strip work-list)");
+  return HL_OK;
+}
+
 template <class S> int stream_tiles(const d2::Launch& L, const TileWork& tw, cudaStream_t st) {
   if (tw.n_tiles == 0) return HL_OK;
   const int x = tw.tile_x, y = tw.tile_y;
+  if (y == d2::STRIP_Y) {
+    if (x == 32) return launch_strips<S, 32>(L, tw, st);
+    if (x == 64) return launch_strips<S, 64>(L, tw, st);
+    if (x == 128) return launch_strips<S, 128>(L, tw, st);
+  }
   if (x == 8 && y == 32) return launch_tiles<S, 8, 32>(L, tw, st);
   if (x == 16 && y == 32) return launch_tiles<S, 16, 32>(L, tw, st);
   if (x == 4 && y == 64) return launch_tiles<S, 4, 64>(L, tw, st);

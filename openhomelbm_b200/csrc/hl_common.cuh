@@ -293,9 +293,10 @@ __device__ __forceinline__ void encode2(const Mom2<typename S::R>& m, const Scal
     raw[0] = m.drho;
     raw[1] = m.ux * sc.inv_u;
     raw[2] = m.uy * sc.inv_u;
-    raw[3] = (m.sxx - m.ux * m.ux) * sc.inv_s;
-    raw[4] = (m.syy - m.uy * m.uy) * sc.inv_s;
-    raw[5] = (m.sxy - m.ux * m.uy) * sc.inv_s;
+    // S - u u as one fused multiply-add, written out so that no kernel's surroundings change it
+    raw[3] = fmaf(-m.ux, m.ux, m.sxx) * sc.inv_s;
+    raw[4] = fmaf(-m.uy, m.uy, m.syy) * sc.inv_s;
+    raw[5] = fmaf(-m.ux, m.uy, m.sxy) * sc.inv_s;
   } else {
     raw[0] = m.rho;
     raw[1] = m.ux;

@@ -11,10 +11,11 @@ from openhomelbm_b200 import batching
 def test_tile_shapes_listed():
     shapes = batching.tile_shapes()
     assert (16, 32) in shapes and len(shapes) == len(set(shapes)) >= 4
-    assert all(tx >= 1 and ty >= 32 for tx, ty in shapes)
+    assert all(tx >= 1 and ty >= 30 for tx, ty in shapes)
+    assert (64, 30) in shapes  # strips: a warp per 30-row tile
 
 
-@pytest.mark.parametrize("shape", [(8, 32), (16, 64), (8, 128)])
+@pytest.mark.parametrize("shape", [(8, 32), (16, 64), (8, 128), (64, 30)])
 def test_tile_list_covers_every_cell_once(shape):
     sizes = [(37, 29), (130, 70), (64, 64), (1, 1)][:3] + [(300, 129)]
     nx, ny = [s[0] for s in sizes], [s[1] for s in sizes]
