@@ -445,12 +445,29 @@ __global__ void __launch_bounds__(256) stream_strips_kernel(const __grid_constan
     // incoming populations of the last two source planes: c_x = 0 (i = 0, 3, 4) of the previous
     // plane, c_x = +1 (i = 1, 5, 8) of the previous two
     R z0 = R(0), z3 = R(0), z4 = R(0), p1 = R(0), p5 = R(0), p8 = R(0), q1 = R(0), q5 = R(0), q8 = R(0);
-    for (int xs = x0 - 1; xs <= x1; ++xs) {
+    // the next source plane's stored moments are loaded one plane ahead
+    auto fetch = [&](int xs, T* t) {
       const int xw = periodic ? wrap(xs, nx) : xs;
+      if (y_in && (periodic || (xs >= 0 && xs < nx))) {
+        const long long c = (long long)xw * ny + y;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) t[k] = cur[k * N + c];
+      }
+    };
+    T tn[6];
+    fetch(x0 - 1, tn);
+    for (int xs = x0 - 1; xs <= x1; ++xs) {
       const bool in = y_in && (periodic || (xs >= 0 && xs < nx));
+      T tc[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) tc[k] = tn[k];
+      if (xs < x1) fetch(xs + 1, tn);
       R f[9];
       if (in) {
-        const Mom2<R> m = load2<S>(wd, N, (long long)xw * ny + y, cur);
+        R raw[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) raw[k] = S::to_r(tc[k]);
+        const Mom2<R> m = decode2<S>(raw, sc);
         const R axxy = third_xxy<R>(m), axyy = third_xyy<R>(m);
 #pragma unroll
         for (int i = 0; i < 9; ++i) f[i] = feq_dev_clamped_a<R>(m, axxy, axyy, i);
