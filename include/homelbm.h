@@ -434,7 +434,9 @@ HL_API int hl_d2q9_step_batch(const void* desc_dev, int n_worlds, int parity, hl
  * launch over a tile work-list (no reference counterpart; it replaces the per-world
  * stream_and_collide launches of LBM_Solver.step, lbm_solver.py:117-139, for uneven worlds).
  * hl_d2q9_tile_shapes writes the supported tile shapes (tile_x, tile_y pairs, at most cap)
- * and returns their number. hl_d2q9_tile_list (host only, no GPU) writes the tiles of n_worlds
+ * and returns their number. Shapes with tile_y = 30 are strips: one warp per tile marches its
+ * 30 rows along x and exchanges populations by warp shuffles (ctas counts blocks of 8 warps);
+ * the others stage a tile in shared memory (ctas counts CTAs of 256 threads). hl_d2q9_tile_list (host only, no GPU) writes the tiles of n_worlds
  * worlds of nx[w] x ny[w] cells, world-major, 4 int32 per tile (world, x0, y0, 0), into out
  * (NULL: count only) and their number into *n_tiles; HL_ERR_ARG if they do not fit in
  * cap_tiles. hl_d2q9_step_tiles runs hl_d2q9_step_batch's phases with the stream phase taken
