@@ -403,10 +403,10 @@ def tgv_diagnostics(f, n):
     return ke, ens
 
 
-def run_precision(args):
+def run_precision(args, n=None, steps=None, every=10):
     """The precision form: the Taylor-Green vortex with float64 (the accuracy oracle, same
     kernels in binary64), float32, float16 and bfloat16 storage. Each run records kinetic
-    energy and enstrophy every 10 steps and the binary64 mass sum every step; the reduced
+    energy and enstrophy every ``every`` steps and the binary64 mass sum every step; the reduced
     forms report their velocity L2 error against the float64 run and their MLUPS against
     the float32 run (timed separately, diagnostics off)."""
     import torch
@@ -415,10 +415,11 @@ def run_precision(args):
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    n, steps, u0 = args.n, args.steps, 0.04
+    n = args.n if n is None else n
+    steps = args.steps if steps is None else steps
+    u0 = 0.04
     vis = u0 * (n / (2 * np.pi)) / 1600.0
     cells = n ** 3
-    every = 10
     res, u_ref = {}, None
     for storage in ("float64", "float32", "float16", "bfloat16"):
         s = LBM_Solver3D(n, n, n, solid_num=1, periodic=True, storage=storage, device=dev, u_scale=u0,
@@ -440,7 +441,8 @@ def run_precision(args):
                 ens.append(ee)
         s.diagnostics = False
         u = f.decoded()[1:4].double()
-        rec = {"ke_every_10": [round(x, 12) for x in ke], "enstrophy_every_10": [round(x, 12) for x in ens],
+        rec = {f"ke_every_{every}": [round(x, 12) for x in ke],
+               f"enstrophy_every_{every}": [round(x, 12) for x in ens],
                "mass_first": float(mass[0]), "mass_last": float(mass[-1]),
                "mass_rel_drift": float((mass[-1] - mass[0]) / mass[0]), "health": int(s.health[0])}
         if u_ref is None:
@@ -487,7 +489,7 @@ def shedding_stats(drag, lift, diameter=24.0, u_in=0.05):
             "period_steps": period, "strouhal": diameter / u_in / period}
 
 
-def run_karman(args):
+def run_karman(args, cpu=True):
     """The D2Q9 Karman configuration: 512 x 128, 96-gon cylinder of radius 12 at (128, 64),
     inflow (0.05, 0), zero gradient elsewhere, nu = 0.012 (Re 100), rho = 1 and u = inflow plus
     seeded +-1e-3 noise. 100000 steps on the GPU with drag and lift recorded every step; the
@@ -533,6 +535,15 @@ def run_karman(args):
     ours = shedding_stats(got[w0:w1, 0], got[w0:w1, 1]) if steps >= w1 else None
     ref = {k: float(g[k]) for k in ("mean_drag", "lift_std", "strouhal", "period_steps")}
     rel = ({k: ours[k] / ref[k] - 1.0 for k in ("mean_drag", "lift_std", "strouhal")} if ours else None)
+    out = {"metric": "D2Q9 Karman wake (512x128, Re 100) Strouhal number vs binary64 oracle",
+           "value": ours["strouhal"] if ours else None, "unit": "St", "higher_is_better": None, "n_gpus": 1,
+           "workload": "karman", "steps": steps, "dtype": "f32", "data": "synthetic (seeded inflow noise)",
+           "window": [w0, w1], "ours": ours, "oracle_f64": ref, "relative_difference": rel,
+           "mlups": nx * ny * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
+           "config": {"workload": "D2Q9 512x128, 96-gon cylinder r=12 at (128,64), inflow 0.05, nu 0.012, bc 0,1,1,1",
+                      "recorded": "drag (solid_forcex) and lift (solid_forcey) every step, device-side"}}
+    if not cpu:
+        return out
     # CPU baseline: the oracle (C++ restatement of the reference kernels, all host threads)
     from oracle import oracle as orc
 
@@ -550,16 +561,10 @@ def run_karman(args):
         mm, pp = new, mm
         n_cpu += 1
     cpu_s = time.perf_counter() - t0
-    return {"metric": "D2Q9 Karman wake (512x128, Re 100) Strouhal number vs binary64 oracle",
-            "value": ours["strouhal"] if ours else None, "unit": "St", "higher_is_better": None, "n_gpus": 1,
-            "workload": "karman", "steps": steps, "dtype": "f32", "data": "synthetic (seeded inflow noise)",
-            "window": [w0, w1], "ours": ours, "oracle_f64": ref, "relative_difference": rel,
-            "mlups": nx * ny * steps / (ms / 1e3) / 1e6, "ms_per_step": ms / steps,
-            "cpu_baseline": {"value": nx * ny * n_cpu / cpu_s / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
-                             "sample": f"{n_cpu} steps of the same 512x128 domain with its cylinder ({cpu_s:.1f} s, "
-                                       "C++ restatement of the reference's D2Q9 kernels, not Warp)"},
-            "config": {"workload": "D2Q9 512x128, 96-gon cylinder r=12 at (128,64), inflow 0.05, nu 0.012, bc 0,1,1,1",
-                       "recorded": "drag (solid_forcex) and lift (solid_forcey) every step, device-side"}}
+    out["cpu_baseline"] = {"value": nx * ny * n_cpu / cpu_s / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
+                           "sample": f"{n_cpu} steps of the same 512x128 domain with its cylinder ({cpu_s:.1f} s, "
+                                     "C++ restatement of the reference's D2Q9 kernels, not Warp)"}
+    return out
 
 
 # ----------------------------------------------------------------------------- serving form
@@ -689,6 +694,30 @@ def run_batch(args):
                        "l2": "inputs larger than L2"}}
 
 
+def karman_leg(args):
+    """configs[0] for the default line: the Karman wake's Strouhal number, mean drag and lift
+    spread over steps 70000-100000 against the binary64 oracle run of the same configuration."""
+    r = run_karman(args, cpu=False)
+    return {k: r[k] for k in ("metric", "value", "unit", "steps", "window", "ours", "oracle_f64",
+                              "relative_difference", "mlups", "config")}
+
+
+def precision_leg(args):
+    """configs[2] for the default line: the Taylor-Green vortex at 512^3 for 2000 steps in float64,
+    float32, float16 and bfloat16 storage; velocity L2 against float64, mass drift, MLUPS, and the
+    kinetic energy every 100 steps."""
+    r = run_precision(args, n=512, steps=2000, every=100)
+    res = {}
+    for st, v in r["results"].items():
+        res[st] = {k: v[k] for k in ("mlups", "mass_rel_drift", "health") if k in v}
+        for k in ("u_l2_vs_float64", "mlups_vs_float32"):
+            if k in v:
+                res[st][k] = v[k]
+        res[st]["ke_every_100"] = v["ke_every_100"]
+    return {"metric": r["metric"], "value": r["value"], "unit": r["unit"], "results": res,
+            "config": dict(r["config"], diagnostics_every=100)}
+
+
 def serve_leg(args):
     """The serving form's figures for the default line: served (float16, continuous batching)
     against the plain float32 solver one request at a time, on the same seeded requests."""
@@ -776,6 +805,12 @@ def main():
                 t0 = time.perf_counter()
                 out["batch"] = batch_leg(args)
                 out["batch"]["leg_wall_s"] = time.perf_counter() - t0
+                t0 = time.perf_counter()
+                out["karman"] = karman_leg(args)
+                out["karman"]["leg_wall_s"] = time.perf_counter() - t0
+                t0 = time.perf_counter()
+                out["precision"] = precision_leg(args)
+                out["precision"]["leg_wall_s"] = time.perf_counter() - t0
         if rank == 0 and out is not None:
             print(json.dumps(out), flush=True)
     finally:
