@@ -414,8 +414,8 @@ __global__ void __launch_bounds__(TILE_THREADS) stream_tiles_kernel(const __grid
 // y0 .. y0 + 29 collide and store it with stream_kernel's collide and store. No shared memory and
 // no block barrier; a strip needs 32/30 of the source work of its cells. Results are identical to
 // stream_kernel. The 32-plane strips with 2- or 4-byte storage are held to 64 registers (four
-// blocks of 8 warps per SM): measured 6 % faster on a 64-world float16 batch, where the 64-plane
-// strips at that cap ran 5 % slower and binary64 storage spills 208 bytes.
+// blocks of 8 warps per SM instead of three), which is faster for them; the 64- and 128-plane
+// strips run slower at that cap, and binary64 storage would spill heavily.
 constexpr int STRIP_Y = 30;
 template <class S, int TX>
 constexpr int strip_min_blocks() { return TX == 32 && sizeof(typename S::T) <= 4 ? 4 : 1; }

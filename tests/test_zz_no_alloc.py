@@ -175,3 +175,40 @@ def test_noalloc_back_to_back_on_one_stream():
         assert _close(out[k].item(), mass), (k, out[k].item(), mass)
         assert bad[k].item() == health == 0, (k, bad[k].item(), health)
     assert out[0].item() != 0.0 and out[1].item() != 0.0
+
+
+def test_noalloc_captured_in_a_graph_after_a_first_call():
+    """The documented order: a first call outside any capture resolves the array's address;
+    a later call may then be captured in a CUDA graph. Each replay writes the same field, mass
+    and health as a direct call on the same input."""
+    shape = (24, 16, 32)
+    lib, code, a, b, flag, force = _setup(shape, "float32", True, False)
+    c = torch.empty_like(a)
+    direct = torch.empty_like(a)
+    st = _lib.stream_ptr()
+    out = torch.zeros(3, dtype=torch.float64, device="cuda")
+    bad = torch.full((3,), -1, dtype=torch.int32, device="cuda")
+    # first call, uncaptured: a -> b
+    _lib.check(lib.hl_d3q27_stream_collide_noalloc(ctypes.byref(_world(shape, code, a, b, True)), 0.01,
+                                                   out[0:].data_ptr(), bad[0:].data_ptr(), st), "noalloc 1")
+    # the reference second step, uncaptured: b -> direct
+    _lib.check(lib.hl_d3q27_stream_collide_noalloc(ctypes.byref(_world(shape, code, b, direct, True)), 0.01,
+                                                   out[1:].data_ptr(), bad[1:].data_ptr(), st), "noalloc 2")
+    torch.cuda.synchronize()
+    w = _world(shape, code, b, c, True)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        _lib.check(lib.hl_d3q27_stream_collide_noalloc(ctypes.byref(w), 0.01, out[2:].data_ptr(),
+                                                       bad[2:].data_ptr(), _lib.stream_ptr()), "noalloc captured")
+    for replay in range(2):
+        c.fill_(float("nan"))
+        out[2] = 0.0
+        bad[2] = -1
+        g.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(c, direct), replay
+        assert out[2].item() == out[1].item(), (replay, out[2].item(), out[1].item())
+        assert bad[2].item() == bad[1].item() == 0, replay
+    mass, health = _expected_diag(c, None)
+    assert _close(out[2].item(), mass) and health == 0
+    del g
