@@ -180,6 +180,24 @@ HL_API int hl_d3q27_stream_collide_batch(const void* desc, int n_domains, int n_
                                          const hl_storage* storage, int parity, int* status, hl_stream stream);
 HL_API size_t hl_d3q27_bc_scratch_bytes(const hl_world3d* w);
 
+/* Batched boundaries (the serving form's batched substep; no reference counterpart: the
+ * reference runs apply_bc_3d per world, envs/lbm3d/lbm_solver_3d.py:88-127). The three waves
+ * of hl_d3q27_apply_bc run as three launches over all domains of a set instead of three per
+ * domain; per cell the same result as hl_d3q27_apply_bc on each domain.
+ *  - hl_d3q27_bc_batch_bytes: device bytes of the descriptors of n domains.
+ *  - hl_d3q27_bc_batch_prepare: writes the descriptors of worlds[0 .. n) (given at parity 0:
+ *    the step reads cur and writes post), their conditions bcs[i] and boundary scratch
+ *    scratch[i] (hl_d3q27_bc_scratch_bytes each, one per domain) into desc (device memory,
+ *    16-byte aligned). Every world walled with sides >= 3, one storage type. Synchronises the
+ *    stream (not for stream capture); prepare again after a domain's buffers change.
+ *  - hl_d3q27_apply_bc_batch: the boundary pass of every domain at parity p (parity 0 writes
+ *    each world's post, parity 1 its cur buffer). n_domains must be the prepared one.
+ *    Capturable. */
+HL_API size_t hl_d3q27_bc_batch_bytes(int n_domains);
+HL_API int hl_d3q27_bc_batch_prepare(const hl_world3d* worlds, const hl_bc3d* bcs, void* const* scratch,
+                                     int n_domains, void* desc, size_t desc_bytes, hl_stream stream);
+HL_API int hl_d3q27_apply_bc_batch(const void* desc, int n_domains, int parity, hl_stream stream);
+
 /* Replaces InitFlow3D (envs/lbm3d/lbm_func_3d.py:22-83) and set_uniform_flow_3d_kernel
  * (envs/lbm3d/karman/karman_lbm_env_3d.py:15-64): rho = 1, u = (ux, uy, uz), S from the
  * equilibrium populations with the reference's cs2_local quirk, forces zeroed, written to

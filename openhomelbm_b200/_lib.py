@@ -115,6 +115,10 @@ _SIGS = {
     "hl_d3q27_stream_collide_batch": ([c_void_p, c_int, c_int, c_double, POINTER(hl_storage), c_int, c_void_p,
                                        c_void_p], c_int),
     "hl_d3q27_bc_scratch_bytes": ([POINTER(hl_world3d)], c_size_t),
+    "hl_d3q27_bc_batch_bytes": ([c_int], c_size_t),
+    "hl_d3q27_bc_batch_prepare": ([POINTER(hl_world3d), POINTER(hl_bc3d), POINTER(c_void_p), c_int, c_void_p, c_size_t,
+                                   c_void_p], c_int),
+    "hl_d3q27_apply_bc_batch": ([c_void_p, c_int, c_int, c_void_p], c_int),
     "hl_d3q27_solid_links": ([POINTER(hl_world3d), c_double, POINTER(hl_solids3d), c_void_p], c_int),
     "hl_d3q27_solid_links_work_ints": ([c_int, c_float], c_size_t),
     "hl_couple_body_states": ([c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int),

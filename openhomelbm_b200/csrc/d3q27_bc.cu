@@ -14,6 +14,11 @@
 //   wave 3: the 8 corners, likewise.
 // Face numbering is the reference's: 0 x=0, 1 x=nx-1, 2 y=ny-1, 3 y=0, 4 z=nz-1, 5 z=0.
 
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <vector>
+
 #include "hl_common.cuh"
 
 namespace hl {
@@ -116,15 +121,16 @@ template <class R> __device__ Mom3<R> bc_core(const BcArgs& a, int dr, const Mom
   return r;
 }
 
-// Wave 1: cells on exactly one face. blockIdx.y = face id = axis * 2 + side.
-template <class S> __global__ void wave1_kernel(const BcArgs a) {
+// Wave 1: cells on exactly one face, face fid = axis * 2 + side; this thread's cells are
+// first, first + stride, ... of the face's interior.
+template <class S> __device__ __forceinline__ void wave1_face(const BcArgs& a, int fid, long long first, long long stride) {
   using T = typename S::T;
-  const int fid = blockIdx.y, ax = fid >> 1, side = fid & 1;
+  const int ax = fid >> 1, side = fid & 1;
   const int b = ax == 0 ? 1 : 0, c = ax == 2 ? 1 : 2;  // the other axes, increasing
   const int nb = a.n[b] - 2, nc = a.n[c] - 2;
   if (nb <= 0 || nc <= 0) return;
   const long long total = (long long)nb * nc;
-  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+  for (long long k = first; k < total; k += stride) {
     int cell[3], nbr[3];
     cell[ax] = side ? a.n[ax] - 1 : 0;
     cell[b] = 1 + int(k / nc);
@@ -143,14 +149,14 @@ template <class S> __global__ void wave1_kernel(const BcArgs a) {
   }
 }
 
-// Wave 2: cells on exactly two faces. blockIdx.y = edge id = free axis * 4 + s1 * 2 + s2,
-// (s1, s2) the sides on the two face axes in increasing order.
-template <class S> __global__ void wave2_kernel(const BcArgs a) {
+// Wave 2: cells on exactly two faces, edge eid = free axis * 4 + s1 * 2 + s2, (s1, s2) the
+// sides on the two face axes in increasing order; cells first, first + stride, ... of the edge.
+template <class S> __device__ __forceinline__ void wave2_edge(const BcArgs& a, int eid, int first, int stride) {
   using T = typename S::T;
-  const int eid = blockIdx.y, a3 = eid >> 2, s1 = (eid >> 1) & 1, s2 = eid & 1;
+  const int a3 = eid >> 2, s1 = (eid >> 1) & 1, s2 = eid & 1;
   const int a1 = a3 == 0 ? 1 : 0, a2 = a3 == 2 ? 1 : 2;
   const int len = a.n[a3] - 2;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < len; k += gridDim.x * blockDim.x) {
+  for (int k = first; k < len; k += stride) {
     int cell[3];
     cell[a1] = s1 ? a.n[a1] - 1 : 0;
     cell[a2] = s2 ? a.n[a2] - 1 : 0;
@@ -178,10 +184,9 @@ template <class S> __global__ void wave2_kernel(const BcArgs a) {
   }
 }
 
-// Wave 3: the 8 corners, one thread each (corner bits x, y, z sides).
-template <class S> __global__ void wave3_kernel(const BcArgs a) {
+// Wave 3: corner k of the 8 (corner bits x, y, z sides).
+template <class S> __device__ __forceinline__ void wave3_corner(const BcArgs& a, int k) {
   using T = typename S::T;
-  const int k = threadIdx.x;
   if (k >= 8) return;
   const int sd[3] = {(k >> 2) & 1, (k >> 1) & 1, k & 1};
   int cell[3];
@@ -205,7 +210,31 @@ template <class S> __global__ void wave3_kernel(const BcArgs a) {
   store_cell<S>(a, i, t);
 }
 
-template <class S> int launch_bc(const hl_world3d* w, const hl_bc3d* bc, void* scratch, cudaStream_t st) {
+// One world: blockIdx.y = face / edge.
+template <class S> __global__ void wave1_kernel(const BcArgs a) {
+  wave1_face<S>(a, blockIdx.y, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
+template <class S> __global__ void wave2_kernel(const BcArgs a) {
+  wave2_edge<S>(a, blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+template <class S> __global__ void wave3_kernel(const BcArgs a) { wave3_corner<S>(a, threadIdx.x); }
+
+// Many worlds: args[2 * w + parity] are world w's arguments at that parity, blockIdx.z (waves
+// 1 and 2) or blockIdx.x (wave 3) the world.
+template <class S> __global__ void wave1_batch_kernel(const BcArgs* __restrict__ args, int parity) {
+  wave1_face<S>(args[2 * blockIdx.z + parity], blockIdx.y, blockIdx.x * (long long)blockDim.x + threadIdx.x,
+                (long long)gridDim.x * blockDim.x);
+}
+template <class S> __global__ void wave2_batch_kernel(const BcArgs* __restrict__ args, int parity) {
+  wave2_edge<S>(args[2 * blockIdx.z + parity], blockIdx.y, blockIdx.x * blockDim.x + threadIdx.x,
+                gridDim.x * blockDim.x);
+}
+template <class S> __global__ void wave3_batch_kernel(const BcArgs* __restrict__ args, int parity) {
+  wave3_corner<S>(args[2 * blockIdx.x + parity], threadIdx.x);
+}
+
+// The boundary pass's arguments for world w, writing w->post.
+BcArgs make_bc_args(const hl_world3d* w, const hl_bc3d* bc, void* scratch) {
   BcArgs a{};
   a.post = w->post;
   a.N = (long long)w->nx * w->ny * w->nz;
@@ -219,15 +248,42 @@ template <class S> int launch_bc(const hl_world3d* w, const hl_bc3d* bc, void* s
   a.sc = make_scale(w->storage);
   a.snap = scratch;
   a.maxn = w->nx > w->ny ? (w->nx > w->nz ? w->nx : w->nz) : (w->ny > w->nz ? w->ny : w->nz);
-  const int maxface = a.maxn * a.maxn;
-  int g1 = (maxface + 255) / 256;
-  if (g1 > 1024) g1 = 1024;
-  wave1_kernel<S><<<dim3(g1, 6), 256, 0, st>>>(a);
+  return a;
+}
+
+// wave 1 blocks per face for faces of up to maxn x maxn cells (grid-stride beyond 1024)
+int wave1_blocks(int maxn) {
+  const long long g = ((long long)maxn * maxn + 255) / 256;
+  return int(g > 1024 ? 1024 : g);
+}
+
+template <class S> int launch_bc(const hl_world3d* w, const hl_bc3d* bc, void* scratch, cudaStream_t st) {
+  const BcArgs a = make_bc_args(w, bc, scratch);
+  wave1_kernel<S><<<dim3(wave1_blocks(a.maxn), 6), 256, 0, st>>>(a);
   HL_LAUNCH_CHECK("d3q27 apply_bc wave 1");
   wave2_kernel<S><<<dim3((a.maxn + 127) / 128, 12), 128, 0, st>>>(a);
   HL_LAUNCH_CHECK("d3q27 apply_bc wave 2");
   wave3_kernel<S><<<1, 32, 0, st>>>(a);
   HL_LAUNCH_CHECK("d3q27 apply_bc wave 3");
+  return HL_OK;
+}
+
+// Prepared batch descriptors: address -> (worlds, storage type, largest side).
+struct BcBatchInfo {
+  int n;
+  hl_dtype dtype;
+  int maxn;
+};
+std::mutex g_bcb_mu;
+std::map<const void*, BcBatchInfo> g_bcb;
+
+template <class S> int launch_bc_batch(const BcArgs* args, const BcBatchInfo& b, int parity, cudaStream_t st) {
+  wave1_batch_kernel<S><<<dim3(wave1_blocks(b.maxn), 6, b.n), 256, 0, st>>>(args, parity);
+  HL_LAUNCH_CHECK("d3q27 apply_bc batch wave 1");
+  wave2_batch_kernel<S><<<dim3((b.maxn + 127) / 128, 12, b.n), 128, 0, st>>>(args, parity);
+  HL_LAUNCH_CHECK("d3q27 apply_bc batch wave 2");
+  wave3_batch_kernel<S><<<b.n, 32, 0, st>>>(args, parity);
+  HL_LAUNCH_CHECK("d3q27 apply_bc batch wave 3");
   return HL_OK;
 }
 
@@ -347,6 +403,67 @@ extern "C" int hl_d3q27_apply_bc(const hl_world3d* w, const hl_bc3d* bc, void* s
     case HL_BF16: return d3bc::launch_bc<StoreBF16>(w, bc, scratch, st);
   }
   set_error("apply_bc_3d: bad dtype");
+  return HL_ERR_ARG;
+}
+
+extern "C" size_t hl_d3q27_bc_batch_bytes(int n_domains) {
+  return n_domains > 0 ? size_t(2) * size_t(n_domains) * sizeof(d3bc::BcArgs) : 0;
+}
+
+extern "C" int hl_d3q27_bc_batch_prepare(const hl_world3d* worlds, const hl_bc3d* bcs, void* const* scratch,
+                                         int n_domains, void* desc, size_t desc_bytes, hl_stream stream) {
+  HL_CHECK_ARG(worlds != nullptr && bcs != nullptr && scratch != nullptr && desc != nullptr,
+               "apply_bc_3d batch: NULL argument");
+  HL_CHECK_ARG(n_domains > 0 && n_domains <= 65535, "apply_bc_3d batch: n_domains must be in 1..65535");
+  const size_t bytes = hl_d3q27_bc_batch_bytes(n_domains);
+  HL_CHECK_ARG(desc_bytes >= bytes, "apply_bc_3d batch: desc_bytes below hl_d3q27_bc_batch_bytes");
+  HL_CHECK_ARG(reinterpret_cast<uintptr_t>(desc) % 16 == 0, "apply_bc_3d batch: desc not 16-byte aligned");
+  const hl_dtype dtype = worlds[0].storage.dtype;
+  std::vector<d3bc::BcArgs> host(size_t(2) * n_domains);
+  int maxn = 0;
+  for (int i = 0; i < n_domains; ++i) {
+    const hl_world3d& w = worlds[i];
+    HL_CHECK_ARG(!w.periodic, "apply_bc_3d batch: world %d is periodic (no boundary pass)", i);
+    HL_CHECK_ARG(w.nx >= 3 && w.ny >= 3 && w.nz >= 3, "apply_bc_3d batch: world %d needs every side >= 3", i);
+    HL_CHECK_ARG(w.storage.dtype == dtype, "apply_bc_3d batch: world %d has another storage type", i);
+    HL_CHECK_ARG(w.cur != nullptr && w.post != nullptr && scratch[i] != nullptr,
+                 "apply_bc_3d batch: world %d has a NULL buffer or scratch", i);
+    // parity 0 writes post, parity 1 the other buffer (the step then reads post)
+    d3bc::BcArgs a = d3bc::make_bc_args(&w, &bcs[i], scratch[i]);
+    host[2 * i] = a;
+    a.post = const_cast<void*>(w.cur);
+    host[2 * i + 1] = a;
+    maxn = std::max(maxn, a.maxn);
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemcpyAsync(desc, host.data(), bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host staging buffer ends here
+  if (e != cudaSuccess) return cuda_status(e, "apply_bc_3d batch: descriptor upload");
+  std::lock_guard<std::mutex> lock(d3bc::g_bcb_mu);
+  d3bc::g_bcb[desc] = d3bc::BcBatchInfo{n_domains, dtype, maxn};
+  return HL_OK;
+}
+
+extern "C" int hl_d3q27_apply_bc_batch(const void* desc, int n_domains, int parity, hl_stream stream) {
+  HL_CHECK_ARG(desc != nullptr, "apply_bc_3d batch: desc is NULL");
+  HL_CHECK_ARG(parity == 0 || parity == 1, "apply_bc_3d batch: parity must be 0 or 1");
+  d3bc::BcBatchInfo b;
+  {
+    std::lock_guard<std::mutex> lock(d3bc::g_bcb_mu);
+    auto it = d3bc::g_bcb.find(desc);
+    HL_CHECK_ARG(it != d3bc::g_bcb.end(), "apply_bc_3d batch: desc was not prepared");
+    b = it->second;
+  }
+  HL_CHECK_ARG(n_domains == b.n, "apply_bc_3d batch: n_domains %d differs from the prepared %d", n_domains, b.n);
+  const auto* args = static_cast<const d3bc::BcArgs*>(desc);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  switch (b.dtype) {
+    case HL_F32: return d3bc::launch_bc_batch<StoreF32>(args, b, parity, st);
+    case HL_F64: return d3bc::launch_bc_batch<StoreF64>(args, b, parity, st);
+    case HL_F16: return d3bc::launch_bc_batch<StoreF16>(args, b, parity, st);
+    case HL_BF16: return d3bc::launch_bc_batch<StoreBF16>(args, b, parity, st);
+  }
+  set_error("apply_bc_3d batch: bad dtype");
   return HL_ERR_ARG;
 }
 

@@ -12,13 +12,12 @@ copies for all substeps) is captured once into a CUDA graph at admission and eac
 launches every active domain's graph on its own CUDA stream, so the domains' kernels overlap
 on the device. With ``batched=True`` each substep is instead ONE stream-collide launch over
 every active domain (hl_d3q27_stream_collide_batch: the tiles of all domains share the SMs)
-and ONE cut-link pass over all of them (hl_d3q27_solid_links_batch), then each domain's
-boundaries and next pose on its own stream; once the
-set of active domains has held for two ticks, the whole control step of the set is one CUDA
-graph (``TickGraph``). Both give the same results; the batched form's stream-collide is
-faster, but its cut links and boundaries then run between two batched launches instead of
-behind other domains' stream-collides, and on B200 the two forms measure within a few
-percent of each other. The poses of every domain's next control step are computed on the host
+and ONE cut-link pass over all of them (hl_d3q27_solid_links_batch), then the boundaries of
+all of them as one launch per wave (hl_d3q27_apply_bc_batch), then each domain's next pose on
+its own stream; once the set of active domains has held for two ticks, the whole control step
+of the set is one CUDA graph (``TickGraph``). Both give the same results; in the batched form
+the cut links and boundaries run between two batched stream-collides instead of behind other
+domains' stream-collides. The poses of every domain's next control step are computed on the host
 while the tick runs on the device. Admission (allocation, initial state, graph capture)
 happens between ticks and counts in the wall time, not in a control step's latency.
 ``run_plain`` is the baseline: the same requests one at a time through the plain drop-in
@@ -238,8 +237,10 @@ class Domain:
             if self.batched:
                 self.pre_graph = self._capture(lambda: self._pose(0))
                 S = req.substeps
-                # what follows the batched stream-collide and cut links of substep k
-                self.post_graphs = [self._capture(lambda k=k: self._after_links(k, k + 1 < S)) for k in range(S)]
+                # what follows the batched stream-collide, cut links and boundaries of substep k:
+                # the pose of substep k + 1 (nothing after the last substep)
+                self.post_graphs = [self._capture(lambda k=k: self._pose(k + 1)) if k + 1 < S else None
+                                    for k in range(S)]
             else:
                 self.graph = self._capture(self._control_step)
         self.event = torch.cuda.Event()
@@ -271,12 +272,6 @@ class Domain:
         if next_pose:
             self._pose(k + 1)
 
-    def _after_links(self, k: int, next_pose: bool) -> None:
-        """Substep k after its batched stream-collide and cut links: boundaries and the pose of
-        substep k + 1."""
-        self.solver._launch(k % 2, _lib.stream_ptr(), stream_collide=False, solid_links=False)
-        if next_pose:
-            self._pose(k + 1)
 
     def _control_step(self) -> None:
         """One control step on the current stream: per substep, the swimmer's pose and one LBM
@@ -320,11 +315,12 @@ class Domain:
             self.ready.record(self.stream)
 
     def after(self, k: int, stream_collide_done: torch.cuda.Event) -> None:
-        """Substep k's part after the batched stream-collide (which ``stream_collide_done``
-        marks); records ``ready``."""
+        """Substep k's part after the batched stream-collide, cut links and boundaries (which
+        ``stream_collide_done`` marks): the pose of substep k + 1; records ``ready``."""
         self.stream.wait_event(stream_collide_done)
         with torch.cuda.stream(self.stream):
-            self.post_graphs[k].replay()
+            if self.post_graphs[k] is not None:
+                self.post_graphs[k].replay()
             self.ready.record(self.stream)
 
     def end(self) -> None:
@@ -422,17 +418,42 @@ class LinkBatch:
             "batched cut links")
 
 
+class BcBatch:
+    """The boundaries of a set of domains as three launches, one per wave, over all of them
+    (hl_d3q27_apply_bc_batch) instead of three per domain. The descriptors cover both
+    parities; each domain keeps its own boundary scratch."""
+
+    def __init__(self, domains: List[Domain], stream: torch.cuda.Stream):
+        L = _lib.lib()
+        flows = [d.solver.flows[0] for d in domains]
+        self.n = len(domains)
+        nbytes = int(L.hl_d3q27_bc_batch_bytes(self.n))
+        worlds = (_lib.hl_world3d * self.n)(*[f.world_struct(0) for f in flows])
+        bcs = (_lib.hl_bc3d * self.n)(*[f.bc_struct() for f in flows])
+        scratch = (ctypes.c_void_p * self.n)(*[_lib.ptr(d.solver._bc_scratch[0]) for d in domains])
+        self.buf = torch.empty(nbytes + 16, dtype=torch.uint8, device=flows[0].device)
+        self.ptr = (self.buf.data_ptr() + 15) // 16 * 16
+        _lib.check(L.hl_d3q27_bc_batch_prepare(worlds, bcs, scratch, self.n, self.ptr, nbytes, _lib.stream_ptr(stream)),
+                   "batched boundaries (prepare)")
+
+    def launch(self, parity: int, stream: torch.cuda.Stream) -> None:
+        _lib.check(_lib.lib().hl_d3q27_apply_bc_batch(self.ptr, self.n, int(parity), _lib.stream_ptr(stream)),
+                   "batched boundaries")
+
+
 class TickGraph:
     """One control step of a fixed set of batched domains as ONE CUDA graph: the pose of
-    substep 0 of every domain, then per substep the batched stream-collide and cut links (the
-    latter per domain when ``links`` is None) followed by every domain's boundaries and next
-    pose, each domain on its own branch.
+    substep 0 of every domain, then per substep the batched stream-collide, cut links and
+    boundaries (the cut links and boundaries per domain when ``links`` is None) followed by
+    every domain's next pose, each domain on its own branch.
     Replaying it costs the host one launch instead of a few calls per domain and substep (which
     leave the device idle between substeps). The pose upload and load download stay outside, on
     the replaying stream."""
 
     def __init__(self, domains: List[Domain], batch: "BatchStep", main: torch.cuda.Stream,
-                 links: Optional[LinkBatch] = None):
+                 links: Optional[LinkBatch] = None, bcs: Optional[BcBatch] = None):
+        if (links is None) != (bcs is None):
+            raise ValueError("TickGraph: batched cut links and batched boundaries go together")
         S = domains[0].req.substeps
         torch.cuda.synchronize()
         fork = torch.cuda.Event()
@@ -452,14 +473,15 @@ class TickGraph:
                 batch.launch(k % 2, main)
                 if links is not None:
                     links.launch(k, main)
+                    bcs.launch(k % 2, main)
                 sc_done[k].record(main)
                 for d, rd in zip(domains, ready):
                     d.stream.wait_event(sc_done[k])
                     with torch.cuda.stream(d.stream):
-                        if links is not None:
-                            d._after_links(k, k + 1 < S)
-                        else:
+                        if links is None:
                             d._after_stream_collide(k, k + 1 < S)
+                        elif k + 1 < S:
+                            d._pose(k + 1)
                     rd[k + 1].record(d.stream)
             for rd in ready:
                 main.wait_event(rd[S])
@@ -571,7 +593,7 @@ class ServeEngine:
         main = torch.cuda.Stream(device=self.device)
         sc_done = torch.cuda.Event()
         tick_done = torch.cuda.Event()
-        batch, links, batch_ids, tick_graph, stable = None, None, None, None, 0
+        batch, links, bcs, batch_ids, tick_graph, stable = None, None, None, None, None, 0
         while pending or active or prepared:
             admit()
             if not active:
@@ -583,6 +605,7 @@ class ServeEngine:
                 if batch_ids != [id(d) for d in running]:
                     batch = BatchStep(running, main)  # the set changed: new descriptors
                     links = LinkBatch(running, main)
+                    bcs = BcBatch(running, main)
                     batch_ids = [id(d) for d in running]
                     tick_graph, stable = None, 0
                 else:
@@ -590,7 +613,7 @@ class ServeEngine:
                 # one graph per set, once the set has held for two ticks (while domains arrive
                 # or finish every tick, capturing would cost more than it saves)
                 if tick_graph is None and stable >= 2:
-                    tick_graph = TickGraph(running, batch, main, links)
+                    tick_graph = TickGraph(running, batch, main, links, bcs)
             t0 = time.perf_counter()
             if tick_graph is not None:
                 with torch.cuda.stream(main):
@@ -610,6 +633,7 @@ class ServeEngine:
                         main.wait_event(d.ready)
                     batch.launch(k % 2, main)
                     links.launch(k, main)
+                    bcs.launch(k % 2, main)
                     sc_done.record(main)
                     for d in running:
                         d.after(k, sc_done)

@@ -150,3 +150,66 @@ def test_batched_cut_links_equal_per_domain(storage):
         a, b = d.loads_dev[0].double(), loads.double()
         assert b.abs().max() > 0
         assert (a - b).abs().max() <= 1e-6 * b.abs().max(), d.req.side
+
+
+@pytest.mark.parametrize("storage", ["float32", "float16"])
+def test_batched_boundaries_equal_per_domain(storage):
+    """hl_d3q27_apply_bc_batch (three launches over all domains) writes, at both parities,
+    exactly what hl_d3q27_apply_bc writes per domain: worlds of different shapes (odd sides
+    included), random moments, a random boundary type per face (fixed velocity, zero gradient,
+    or a type that keeps the cell's own velocity)."""
+    from openhomelbm_b200 import _lib
+
+    L = _lib.lib()
+    st = _lib.stream_ptr()
+    code = _lib.DTYPES[storage]
+    sto = _lib.hl_storage(code, 0.05, 2e-3) if storage != "float32" else _lib.hl_storage(code, 1.0, 1.0)
+    rng = np.random.default_rng(5)
+    shapes = [(16, 24, 32), (33, 17, 20), (8, 9, 10), (40, 32, 32), (3, 5, 7)]
+    doms = []
+    for nx, ny, nz in shapes:
+        b0 = torch.tensor(rng.uniform(-0.5, 0.5, (10, nx, ny, nz)), dtype=_lib.torch_dtype(code), device="cuda")
+        b1 = torch.tensor(rng.uniform(-0.5, 0.5, (10, nx, ny, nz)), dtype=_lib.torch_dtype(code), device="cuda")
+        if storage == "float32":  # rho near 1
+            b0[0] += 1.0
+            b1[0] += 1.0
+        bc = _lib.hl_bc3d()
+        for f in range(6):
+            bc.bc_type[f] = int(rng.integers(0, 3))
+            for k in range(3):
+                bc.bc_value[f][k] = float(rng.uniform(-0.03, 0.03))
+        w = _lib.hl_world3d(nx, ny, nz, sto, b0.data_ptr(), b1.data_ptr(), None, None, 0)
+        scratch = torch.zeros(int(L.hl_d3q27_bc_scratch_bytes(ctypes.byref(w))), dtype=torch.uint8, device="cuda")
+        doms.append(dict(b=(b0, b1), bc=bc, shape=(nx, ny, nz), scratch=scratch))
+    n = len(doms)
+    nbytes = int(L.hl_d3q27_bc_batch_bytes(n))
+    desc = torch.empty(nbytes + 16, dtype=torch.uint8, device="cuda")
+    ptr = (desc.data_ptr() + 15) // 16 * 16
+    worlds = (_lib.hl_world3d * n)(*[_lib.hl_world3d(*d["shape"], sto, d["b"][0].data_ptr(), d["b"][1].data_ptr(),
+                                                     None, None, 0) for d in doms])
+    bcs = (_lib.hl_bc3d * n)(*[d["bc"] for d in doms])
+    scr = (ctypes.c_void_p * n)(*[d["scratch"].data_ptr() for d in doms])
+    _lib.check(L.hl_d3q27_bc_batch_prepare(worlds, bcs, scr, n, ptr, nbytes, st), "prepare")
+    for parity in (0, 1):
+        start = [d["b"][1 - parity].clone() for d in doms]  # the buffer the pass writes
+        ref = []
+        for d, s0 in zip(doms, start):
+            out = d["b"][1 - parity]
+            out.copy_(s0)
+            cur = d["b"][parity]
+            w = _lib.hl_world3d(*d["shape"], sto, cur.data_ptr(), out.data_ptr(), None, None, 0)
+            _lib.check(L.hl_d3q27_apply_bc(ctypes.byref(w), ctypes.byref(d["bc"]), d["scratch"].data_ptr(), st), "bc")
+            torch.cuda.synchronize()
+            ref.append(out.clone())
+            assert not torch.equal(out, s0)  # the pass changed the border
+            out.copy_(s0)
+        _lib.check(L.hl_d3q27_apply_bc_batch(ptr, n, parity, st), "batched bc")
+        torch.cuda.synchronize()
+        for d, r in zip(doms, ref):
+            assert torch.equal(d["b"][1 - parity], r), (d["shape"], parity)
+    with pytest.raises(ValueError):  # counts that were not prepared
+        _lib.check(L.hl_d3q27_apply_bc_batch(ptr, n + 1, 0, st))
+    with pytest.raises(ValueError):  # a periodic world
+        pw = (_lib.hl_world3d * 1)(_lib.hl_world3d(8, 8, 8, sto, doms[2]["b"][0].data_ptr(),
+                                                   doms[2]["b"][1].data_ptr(), None, None, 1))
+        _lib.check(L.hl_d3q27_bc_batch_prepare(pw, bcs, scr, 1, ptr, nbytes, st))
