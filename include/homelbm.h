@@ -61,8 +61,10 @@ HL_API const char* hl_version(void);
  *   "d3q27_chunks": 0 automatic, k > 0 splits x into k chunks per tile column (read by
  *     hl_d3q27_stream_collide at launch and by hl_d3q27_batch_prepare)
  *   "d3q27_stages": 0 automatic (4), 3..5 planes staged by the TMA kernel
- *   "d3q27_link_blocks": 0 automatic (4 per SM), k > 0 blocks of the cut-link kernel over the
- *     listed cells (fewer leave SMs free for other domains' kernels on other streams)
+ *   "d3q27_link_blocks": 0 automatic, k > 0 blocks of the cut-link kernel over the listed
+ *     cells (fewer leave SMs free for other domains' kernels on other streams): blocks of 16
+ *     warps for hl_d3q27_solid_links (automatic: one per SM), of 4 warps for
+ *     hl_d3q27_solid_links_batch (automatic: four per SM)
  * Returns HL_ERR_ARG for an unknown key. A CUDA graph keeps the choice it was captured with. */
 HL_API int hl_set_tuning(const char* key, int value);
 

@@ -591,14 +591,20 @@ __device__ __forceinline__ void loads_out(const hl_solids3d& s, int k) {
 }
 
 // The block that finishes last (work[1] counts finished blocks) writes the binary32 loads.
-template <class S> __global__ void __launch_bounds__(BLOCK) process_kernel(const __grid_constant__ Args a) {
+// Blocks of 16 warps (one per SM at 104 registers), each warp's scratch in dynamic shared
+// memory: a warp spends most of a cell waiting on dependent loads, so more warps per SM hide
+// more of it than the same warps spread over more SMs.
+constexpr int PBLOCK = 512;
+constexpr int PBLOCK_SMEM = int(sizeof(WarpScratch)) * (PBLOCK / 32);
+template <class S> __global__ void __launch_bounds__(PBLOCK) process_kernel(const __grid_constant__ Args a) {
   __shared__ double acc[MAX_SOLIDS * 6];
   __shared__ bool last;
+  extern __shared__ __align__(16) unsigned char process_smem[];
+  WarpScratch* scratch = reinterpret_cast<WarpScratch*>(process_smem);  // [PBLOCK / 32]
   const hl_solids3d& s = a.s;
   const int n = s.n_objects;
   for (int k = threadIdx.x; k < 6 * n; k += blockDim.x) acc[k] = 0.0;
   __syncthreads();
-  __shared__ WarpScratch scratch[BLOCK / 32];
   const int count = s.work[0];
   const int ny = a.w.ny, nz = a.w.nz;
   bool any = false;
@@ -729,10 +735,12 @@ template <class S> int launch(const hl_world3d* w, double vis, const hl_solids3d
     if (e != cudaSuccess) return cuda_status(e, "d3q27 solid links: zero work count");
     classify_kernel<S><<<grid, BLOCK, 0, st>>>(a);
     HL_LAUNCH_CHECK("d3q27 solid links (classify)");
-    // four blocks per SM, as many as the registers allow (measured: 6 or 8 with fewer
-    // registers spill and run no faster); the last block to finish writes the binary32 loads
-    const int blocks = g_tune_d3_link_blocks > 0 ? g_tune_d3_link_blocks : 4 * num_sms_local();
-    process_kernel<S><<<unsigned(blocks), BLOCK, 0, st>>>(a);
+    // one 16-warp block per SM unless set; the last block to finish writes the binary32 loads
+    const int blocks = g_tune_d3_link_blocks > 0 ? g_tune_d3_link_blocks : num_sms_local();
+    const int ar = set_smem_attr(reinterpret_cast<const void*>(&process_kernel<S>), PBLOCK_SMEM,
+                                 "d3q27 solid links (cut cells)");
+    if (ar != HL_OK) return ar;
+    process_kernel<S><<<unsigned(blocks), PBLOCK, size_t(PBLOCK_SMEM), st>>>(a);
     HL_LAUNCH_CHECK("d3q27 solid links (cut cells)");
   } else {
     band_kernel<S><<<grid, BLOCK, 0, st>>>(a);

@@ -535,11 +535,13 @@ class ServeEngine:
         if self.x_chunks < 0:
             raise ValueError(f"x_chunks must be >= 0, got {x_chunks}")
         # blocks of each domain's cut-link kernel (the library's "d3q27_link_blocks" while run()
-        # lasts; 0 keeps the library's 4 per SM). None: one per SM for per-domain graphs, 0 for
-        # the batched form: with resident domains sharing the GPU, fewer blocks per domain leave
-        # the other domains' kernels room.
+        # lasts; 0 keeps the library's automatic grid). None: a quarter of the SM count for
+        # per-domain graphs (16-warp blocks: 592 warps on a 148-SM B200), 0 for the batched form:
+        # with resident domains sharing the GPU, fewer blocks per domain leave the other domains'
+        # kernels room.
         if link_blocks is None:
-            link_blocks = 0 if self.batched else torch.cuda.get_device_properties(self.device).multi_processor_count
+            sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+            link_blocks = 0 if self.batched else max(1, sms // 4)
         self.link_blocks = int(link_blocks)
         if not 0 <= self.link_blocks <= 4096:
             raise ValueError(f"link_blocks must be in 0..4096, got {link_blocks}")
