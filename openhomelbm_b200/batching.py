@@ -459,7 +459,6 @@ def run_sequential_plain(specs: Sequence[SwimmerSpec], control_steps: int, subst
     """Baseline: the worlds one after another through the plain LBM_Solver (one graph launch
     per LBM step), poses through the 2D coupling kernel, loads read back every control step.
     The wall time is the stepping time of all worlds (each world's set-up excluded)."""
-    from . import coupling  # noqa: F401  (same kernels as the batch's pose update)
     from .lbm import LBM_Solver
 
     dev = _lib.require_cuda(device)

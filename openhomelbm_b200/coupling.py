@@ -11,8 +11,6 @@ synchronises nothing, so a caller can capture it into the step's CUDA graph.
 """
 from __future__ import annotations
 
-from typing import Optional
-
 import torch
 
 from . import _lib

@@ -29,6 +29,7 @@ read and write only that domain's buffers.
 from __future__ import annotations
 
 import contextlib
+import ctypes
 import gc
 import math
 import os
@@ -41,8 +42,6 @@ import torch
 
 from . import _lib
 from .lbm3d import LBM_Solver3D
-
-import ctypes
 
 SEGMENTS = 5
 # One hardware work queue per domain stream: with CUDA's default of 8, the streams of more

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 import torch
 
-from conftest import load_golden, moment_errors as rel_err
+from conftest import load_golden
 from oracle import oracle as orc
 
 pytestmark = pytest.mark.gpu
