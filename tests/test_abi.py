@@ -62,6 +62,19 @@ def test_batch_live_view_and_control_arguments_are_checked_without_the_gpu():
     assert lib.hl_d3q27_solid_links_batch(64, 1, 3, 64, 1 << 20, None) == arg
     assert lib.hl_d3q27_solid_links_batch(64, 1, 0, 64, 1 << 20, None) == arg
     assert b"not prepared" in lib.hl_last_error()
+    assert lib.hl_d3q27_bc_batch_bytes(0) == 0
+    bcs = (_lib.hl_bc3d * 1)()
+    scratch = (ctypes.c_void_p * 1)(64)
+    assert lib.hl_d3q27_bc_batch_prepare(worlds, bcs, scratch, 0, 64, 1 << 20, None) == arg  # no domains
+    assert lib.hl_d3q27_bc_batch_prepare(worlds, bcs, scratch, 1, 64 + 8, 1 << 20, None) == arg
+    assert b"16-byte" in lib.hl_last_error()
+    assert lib.hl_d3q27_bc_batch_prepare(worlds, bcs, scratch, 1, 64, 8, None) == arg
+    assert b"below" in lib.hl_last_error()
+    assert lib.hl_d3q27_bc_batch_prepare(worlds, bcs, scratch, 1, 64, 1 << 20, None) == arg
+    assert b"NULL buffer" in lib.hl_last_error()  # the domain's buffers are NULL
+    assert lib.hl_d3q27_apply_bc_batch(64, 1, 2, None) == arg
+    assert lib.hl_d3q27_apply_bc_batch(64, 1, 0, None) == arg
+    assert b"not prepared" in lib.hl_last_error()
     pos = (ctypes.c_int32 * 1)(3)
     assert lib.hl_d3q27_live_slices(ctypes.byref(w), pos, 1, 8, 8, 1, 0, 0, 0, 0, 64, None, None) == arg  # cur NULL
     w.cur = 64
